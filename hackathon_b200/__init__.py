@@ -1,0 +1,230 @@
+"""B200 (sm_100a) compact Helmholtz direct solver -- Python host mirror of the C ABI.
+
+The product is the in-tree shared library `libhh.so` (CUDA kernels for sm_100a behind the
+C ABI of include/hh.h) and the drop-in libraries `libhh2d.so` / `libhh3d.so` that export the
+reference's own entry points (solver(System), forwardDST, reverseDST, DST).  This module only
+loads `libhh.so` with ctypes and wraps its calls; it has no numerical code of its own and no
+CPU fallback -- if the library or a GPU is missing, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhh.so")
+DROPIN2D_PATH = os.path.join(HERE, "libhh2d.so")
+DROPIN3D_PATH = os.path.join(HERE, "libhh3d.so")
+
+HH_OK = 0
+STATUS = {0: "HH_OK", 1: "HH_ERR_INVALID", 2: "HH_ERR_CUDA", 3: "HH_ERR_NOMEM", 4: "HH_ERR_UNSUPPORTED",
+          5: "HH_ERR_DEVICE"}
+
+# every symbol include/hh.h declares, with its ctypes signature
+_vp, _i, _l, _d, _sz = C.c_void_p, C.c_int, C.c_long, C.c_double, C.c_size_t
+_dp = C.POINTER(C.c_double)
+SIGNATURES = {
+    "hh_last_error": (C.c_char_p, []),
+    "hh_version": (_i, []),
+    "hh_ctx_create": (_i, [_i, _vp, C.POINTER(_vp)]),
+    "hh_ctx_destroy": (_i, [_vp]),
+    "hh_ctx_set_stream": (_i, [_vp, _vp]),
+    "hh_ctx_synchronize": (_i, [_vp]),
+    "hh_ctx_launch_count": (C.c_longlong, [_vp]),
+    "hh_malloc": (_i, [_vp, _sz, C.POINTER(_vp)]),
+    "hh_free": (_i, [_vp, _vp]),
+    "hh_memcpy_h2d": (_i, [_vp, _vp, _vp, _sz]),
+    "hh_memcpy_d2h": (_i, [_vp, _vp, _vp, _sz]),
+    "hh_dst1_rows": (_i, [_vp, _i, _l, _vp, _l, _vp, _l]),
+    "hh_dst1_cols": (_i, [_vp, _i, _l, _l, _vp, _l, _l, _vp]),
+    "hh_dst2_planes": (_i, [_vp, _i, _i, _l, _vp, _vp]),
+    "hh_plan2d_create": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(_vp)]),
+    "hh_plan3d_create": (_i, [_vp, _i, _i, _i, C.POINTER(_vp), C.POINTER(_vp)]),
+    "hh_plan2d_create_helmholtz": (_i, [_vp, _i, _i, _d, _d, C.POINTER(_vp)]),
+    "hh_plan3d_create_helmholtz": (_i, [_vp, _i, _i, _d, _d, C.POINTER(_vp)]),
+    "hh_plan_destroy": (_i, [_vp]),
+    "hh_plan_field_size": (_l, [_vp]),
+    "hh_solve": (_i, [_vp, _vp, _vp, _i]),
+    "hh_solve_host": (_i, [_vp, _vp, _vp, _i]),
+    "hh_solve_source": (_i, [_vp, _vp, _vp, _i]),
+    "hh_solve_source_host": (_i, [_vp, _vp, _vp, _i]),
+    "hh_coefficients2d": (_i, [_i, _i, _d, _d, C.POINTER(_vp)]),
+    "hh_coefficients3d": (_i, [_i, _i, _d, _d, C.POINTER(_vp)]),
+    "hh_ctx_set_stage_timing": (_i, [_vp, _i]),
+    "hh_ctx_stage_times": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
+}
+
+_lib = None
+
+
+class HHError(RuntimeError):
+    pass
+
+
+def lib() -> C.CDLL:
+    """Load libhh.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise HHError(f"{LIB_PATH} is missing; build it with `python -m hackathon_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != HH_OK:
+        msg = lib().hh_last_error().decode(errors="replace")
+        raise HHError(f"{what}: {STATUS.get(rc, rc)}: {msg}")
+
+
+def _addr(buf) -> int:
+    """Device or host address of a torch tensor, a numpy array or an integer."""
+    if isinstance(buf, int):
+        return buf
+    if isinstance(buf, np.ndarray):
+        assert buf.flags["C_CONTIGUOUS"]
+        return buf.ctypes.data
+    if hasattr(buf, "data_ptr"):
+        return buf.data_ptr()
+    raise TypeError(type(buf))
+
+
+class Context:
+    """One device + one CUDA stream (include/hh.h hh_ctx)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        p = _vp()
+        check(lib().hh_ctx_create(device, stream, C.byref(p)), "hh_ctx_create")
+        self.h = p
+        self.device = device
+
+    def close(self):
+        if self.h:
+            lib().hh_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream: int | None):
+        check(lib().hh_ctx_set_stream(self.h, stream), "hh_ctx_set_stream")
+
+    def synchronize(self):
+        check(lib().hh_ctx_synchronize(self.h), "hh_ctx_synchronize")
+
+    def set_stage_timing(self, on: bool):
+        check(lib().hh_ctx_set_stage_timing(self.h, 1 if on else 0), "hh_ctx_set_stage_timing")
+
+    def stage_times(self):
+        """(ms per stage [forward, lines, inverse], solves timed) since the last call."""
+        ms = (C.c_double * 3)()
+        n = C.c_longlong()
+        check(lib().hh_ctx_stage_times(self.h, ms, C.byref(n)), "hh_ctx_stage_times")
+        return list(ms), int(n.value)
+
+    @property
+    def launches(self) -> int:
+        return int(lib().hh_ctx_launch_count(self.h))
+
+    # -- transforms on device buffers (complex128)
+    def dst1_rows(self, n: int, rows: int, src, dst, in_ld: int | None = None, out_ld: int | None = None):
+        check(lib().hh_dst1_rows(self.h, n, rows, _addr(src), in_ld or n, _addr(dst), out_ld or n), "hh_dst1_rows")
+
+    def dst1_cols(self, n: int, ncols: int, planes: int, src, ld: int, plane_stride: int, dst):
+        check(lib().hh_dst1_cols(self.h, n, ncols, planes, _addr(src), ld, plane_stride, _addr(dst)), "hh_dst1_cols")
+
+    def dst2_planes(self, nx: int, ny: int, planes: int, src, dst):
+        check(lib().hh_dst2_planes(self.h, nx, ny, planes, _addr(src), _addr(dst)), "hh_dst2_planes")
+
+
+def _coef_ptrs(arrs):
+    keep = [np.ascontiguousarray(a, dtype=np.complex128) for a in arrs]
+    return keep, (_vp * len(keep))(*[k.ctypes.data for k in keep])
+
+
+class Plan:
+    """A device-resident problem (include/hh.h hh_plan)."""
+
+    def __init__(self, ctx: Context, handle, dim: int, shape: tuple):
+        self.ctx, self.h, self.dim, self.shape = ctx, handle, dim, shape
+        self.field = int(lib().hh_plan_field_size(handle))
+
+    @classmethod
+    def from_coefficients_2d(cls, ctx: Context, nx: int, ny: int, coef: dict):
+        keep = [np.ascontiguousarray(coef[k], dtype=np.complex128) for k in ("bp", "ap", "b", "a", "bm", "am")]
+        p = _vp()
+        check(lib().hh_plan2d_create(ctx.h, nx, ny, *[k.ctypes.data for k in keep], C.byref(p)), "hh_plan2d_create")
+        return cls(ctx, p, 2, (ny, nx))
+
+    @classmethod
+    def from_coefficients_3d(cls, ctx: Context, nx: int, ny: int, nz: int, coef: dict):
+        names = ("a", "b", "c", "d", "ap", "bp", "cp", "dp", "am", "bm", "cm", "dm")
+        keep, arr = _coef_ptrs([coef[k] for k in names])
+        p = _vp()
+        check(lib().hh_plan3d_create(ctx.h, nx, ny, nz, arr, C.byref(p)), "hh_plan3d_create")
+        return cls(ctx, p, 3, (nz, ny, nx))
+
+    @classmethod
+    def helmholtz(cls, ctx: Context, dim: int, n: int, order: int, k: complex):
+        p = _vp()
+        k = complex(k)
+        if dim == 2:
+            check(lib().hh_plan2d_create_helmholtz(ctx.h, n, order, k.real, k.imag, C.byref(p)), "helmholtz2d")
+            return cls(ctx, p, 2, (n, n))
+        check(lib().hh_plan3d_create_helmholtz(ctx.h, n, order, k.real, k.imag, C.byref(p)), "helmholtz3d")
+        return cls(ctx, p, 3, (n, n, n))
+
+    def close(self):
+        if self.h:
+            lib().hh_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- device buffers (torch tensors / raw addresses)
+    def solve(self, rhs, sol, batch: int = 1):
+        check(lib().hh_solve(self.h, _addr(rhs), _addr(sol), batch), "hh_solve")
+
+    def solve_source(self, f, u, batch: int = 1):
+        check(lib().hh_solve_source(self.h, _addr(f), _addr(u), batch), "hh_solve_source")
+
+    # -- host numpy arrays
+    def solve_host(self, rhs: np.ndarray) -> np.ndarray:
+        rhs = np.ascontiguousarray(rhs, dtype=np.complex128)
+        batch = rhs.size // self.field
+        out = np.empty_like(rhs)
+        check(lib().hh_solve_host(self.h, rhs.ctypes.data, out.ctypes.data, batch), "hh_solve_host")
+        return out
+
+    def solve_source_host(self, f: np.ndarray) -> np.ndarray:
+        f = np.ascontiguousarray(f, dtype=np.complex128)
+        batch = f.size // self.field
+        out = np.empty_like(f)
+        check(lib().hh_solve_source_host(self.h, f.ctypes.data, out.ctypes.data, batch), "hh_solve_source_host")
+        return out
+
+
+def coefficients(dim: int, n: int, order: int, k: complex) -> dict:
+    """Stencil coefficients of the constant-k schemes (hh_coefficients2d/3d)."""
+    k = complex(k)
+    names = ("bp", "ap", "b", "a", "bm", "am") if dim == 2 else \
+        ("a", "b", "c", "d", "ap", "bp", "cp", "dp", "am", "bm", "cm", "dm")
+    arrs = [np.zeros(n, dtype=np.complex128) for _ in names]
+    ptrs = (_vp * len(arrs))(*[a.ctypes.data for a in arrs])
+    f = lib().hh_coefficients2d if dim == 2 else lib().hh_coefficients3d
+    check(f(n, order, k.real, k.imag, ptrs), "hh_coefficients")
+    return dict(zip(names, arrs))

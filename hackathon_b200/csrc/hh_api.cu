@@ -1,0 +1,521 @@
+// C ABI (include/hh.h): contexts, plans and the solve pipeline on sm_100a.
+//
+// Pipeline for one batch of right-hand sides (all on the plan's stream, no host round trip):
+//   2D  rhs --DST-I along x (rows)--> F^ --line solves along y--> U^ --DST-I along x--> u
+//   3D  rhs --DST-I x (rows), y (columns)--> F^ --line solves along z--> U^ --DST-I y, x--> u
+// which is the reference's solver() (2D_Program/solver_functions/solver.c:66-90,
+// 3D_Program/solver_functions/solver.c:465-515).  Every stage works in place on the output
+// buffer, so the solve needs no scratch beyond the output itself.
+#include "hh_internal.cuh"
+
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+
+struct hh_ctx {
+    hh::Ctx c;
+};
+struct hh_plan {
+    hh::Plan p;
+    // host staging for hh_solve_host / hh_solve_source_host
+    double2 *stage = nullptr;
+    long     stage_elems = 0;
+};
+
+namespace hh {
+
+static thread_local std::string g_err;
+
+void set_error(const char *fmt, ...) {
+    char    buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line) {
+    set_error("%s failed: %s (%d) at %s:%d", what, cudaGetErrorString(e), (int)e, file, line);
+    return e == cudaErrorMemoryAllocation ? HH_ERR_NOMEM : HH_ERR_CUDA;
+}
+
+static int upload(Ctx *c, void *dst, const void *src, size_t bytes) {
+    HH_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    return HH_OK;
+}
+
+} // namespace hh
+
+using namespace hh;
+
+static void drain_events(Ctx &c);
+
+// ------------------------------------------------------------------ library ------
+extern "C" const char *hh_last_error(void) { return g_err.c_str(); }
+extern "C" int hh_version(void) { return 100; }
+
+// ----------------------------------------------------------------- contexts ------
+extern "C" int hh_ctx_create(int device, void *stream, hh_ctx **out) {
+    if (!out) { set_error("hh_ctx_create: null out"); return HH_ERR_INVALID; }
+    *out = nullptr;
+    int ndev = 0;
+    HH_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) { set_error("hh_ctx_create: device %d of %d", device, ndev); return HH_ERR_INVALID; }
+    HH_CUDA(cudaSetDevice(device));
+    hh_ctx *x = new hh_ctx();
+    x->c.device = device;
+    if (stream) {
+        x->c.stream = (cudaStream_t)stream;
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&x->c.stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { delete x; return cuda_fail(e, "cudaStreamCreateWithFlags", __FILE__, __LINE__); }
+        x->c.own_stream = true;
+    }
+    cudaError_t e = cudaMalloc(&x->c.err_word, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(x->c.err_word, 0, sizeof(int));
+    if (e != cudaSuccess) {
+        if (x->c.own_stream) cudaStreamDestroy(x->c.stream);
+        delete x;
+        return cuda_fail(e, "error word", __FILE__, __LINE__);
+    }
+    *out = x;
+    return HH_OK;
+}
+
+extern "C" int hh_ctx_destroy(hh_ctx *x) {
+    if (!x) return HH_OK;
+    cudaSetDevice(x->c.device);
+    cudaStreamSynchronize(x->c.stream);
+    drain_events(x->c);
+    for (auto &kv : x->c.tw) cudaFree(kv.second);
+    for (auto &kv : x->c.sn) cudaFree(kv.second);
+    for (auto &kv : x->c.dense) cudaFree(kv.second);
+    cudaFree(x->c.err_word);
+    if (x->c.own_stream) cudaStreamDestroy(x->c.stream);
+    delete x;
+    return HH_OK;
+}
+
+extern "C" int hh_ctx_set_stream(hh_ctx *x, void *stream) {
+    if (!x) return HH_ERR_INVALID;
+    if (x->c.own_stream) { cudaStreamDestroy(x->c.stream); x->c.own_stream = false; }
+    x->c.stream = (cudaStream_t)stream;
+    return HH_OK;
+}
+
+extern "C" int hh_ctx_synchronize(hh_ctx *x) {
+    if (!x) return HH_ERR_INVALID;
+    HH_CUDA(cudaSetDevice(x->c.device));
+    HH_CUDA(cudaStreamSynchronize(x->c.stream));
+    int flag = 0;
+    HH_CUDA(cudaMemcpy(&flag, x->c.err_word, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+        HH_CUDA(cudaMemset(x->c.err_word, 0, sizeof(int)));
+        set_error("a kernel reported an expired bounded wait (code %d)", flag);
+        return HH_ERR_DEVICE;
+    }
+    return HH_OK;
+}
+
+extern "C" long long hh_ctx_launch_count(const hh_ctx *x) { return x ? x->c.launches : 0; }
+
+static void drain_events(Ctx &c) {
+    for (size_t g = 0; g + 4 <= c.ev_pending.size(); g += 4) {
+        float t;
+        for (int s = 0; s < 3; s++) {
+            if (cudaEventElapsedTime(&t, c.ev_pending[g + s], c.ev_pending[g + s + 1]) == cudaSuccess)
+                c.stage_ms[s] += t;
+        }
+        for (int s = 0; s < 4; s++) cudaEventDestroy(c.ev_pending[g + s]);
+    }
+    c.ev_pending.clear();
+}
+
+extern "C" int hh_ctx_set_stage_timing(hh_ctx *x, int on) {
+    if (!x) return HH_ERR_INVALID;
+    x->c.timing = on != 0;
+    return HH_OK;
+}
+
+extern "C" int hh_ctx_stage_times(hh_ctx *x, double ms[HH_NUM_STAGES], long long *solves) {
+    if (!x || !ms) return HH_ERR_INVALID;
+    HH_CUDA(cudaStreamSynchronize(x->c.stream));
+    drain_events(x->c);
+    for (int s = 0; s < 3; s++) {
+        ms[s] = x->c.stage_ms[s];
+        x->c.stage_ms[s] = 0.0;
+    }
+    if (solves) *solves = x->c.timed_solves;
+    x->c.timed_solves = 0;
+    return HH_OK;
+}
+
+// records event `k` (0..3) of the current timed solve
+static int stage_mark(Ctx &c, int k) {
+    if (!c.timing) return HH_OK;
+    if (k == 0 && c.ev_pending.size() >= 4 * 64) drain_events(c); // bound the backlog
+    cudaEvent_t e;
+    HH_CUDA(cudaEventCreate(&e));
+    HH_CUDA(cudaEventRecord(e, c.stream));
+    c.ev_pending.push_back(e);
+    if (k == 3) c.timed_solves++;
+    return HH_OK;
+}
+
+extern "C" int hh_malloc(hh_ctx *x, size_t bytes, void **p) {
+    if (!x || !p) return HH_ERR_INVALID;
+    HH_CUDA(cudaSetDevice(x->c.device));
+    HH_CUDA(cudaMalloc(p, bytes));
+    return HH_OK;
+}
+extern "C" int hh_free(hh_ctx *x, void *p) {
+    if (!x) return HH_ERR_INVALID;
+    HH_CUDA(cudaFree(p));
+    return HH_OK;
+}
+extern "C" int hh_memcpy_h2d(hh_ctx *x, void *d, const void *s, size_t n) {
+    if (!x) return HH_ERR_INVALID;
+    HH_CUDA(cudaMemcpyAsync(d, s, n, cudaMemcpyHostToDevice, x->c.stream));
+    HH_CUDA(cudaStreamSynchronize(x->c.stream));
+    return HH_OK;
+}
+extern "C" int hh_memcpy_d2h(hh_ctx *x, void *d, const void *s, size_t n) {
+    if (!x) return HH_ERR_INVALID;
+    HH_CUDA(cudaMemcpyAsync(d, s, n, cudaMemcpyDeviceToHost, x->c.stream));
+    HH_CUDA(cudaStreamSynchronize(x->c.stream));
+    return HH_OK;
+}
+
+// --------------------------------------------------------------- transforms ------
+extern "C" int hh_dst1_rows(hh_ctx *x, int n, long rows, const double *in, long in_ld, double *out, long out_ld) {
+    if (!x || !in || !out || n < 1 || rows < 0 || in_ld < n || out_ld < n) {
+        set_error("hh_dst1_rows: invalid arguments");
+        return HH_ERR_INVALID;
+    }
+    return launch_dst_rows(&x->c, n, rows, (const double2 *)in, in_ld, (double2 *)out, out_ld);
+}
+
+extern "C" int hh_dst1_cols(hh_ctx *x, int n, long ncols, long planes, const double *in, long ld, long plane_stride,
+                            double *out) {
+    if (!x || !in || !out || n < 1 || ncols < 0 || planes < 0 || ld < ncols || planes > 65535) {
+        set_error("hh_dst1_cols: invalid arguments");
+        return HH_ERR_INVALID;
+    }
+    return launch_dst_cols(&x->c, n, ncols, planes, (const double2 *)in, ld, plane_stride, (double2 *)out);
+}
+
+extern "C" int hh_dst2_planes(hh_ctx *x, int nx, int ny, long nplanes, const double *in, double *out) {
+    if (!x || !in || !out || nx < 1 || ny < 1 || nplanes < 0) {
+        set_error("hh_dst2_planes: invalid arguments");
+        return HH_ERR_INVALID;
+    }
+    const long plane = (long)nx * ny;
+    HH_TRY(launch_dst_rows(&x->c, nx, (long)ny * nplanes, (const double2 *)in, nx, (double2 *)out, nx));
+    for (long p0 = 0; p0 < nplanes; p0 += 65535) {
+        const long np = (nplanes - p0 < 65535) ? nplanes - p0 : 65535;
+        double2   *o = (double2 *)out + p0 * plane;
+        HH_TRY(launch_dst_cols(&x->c, ny, nx, np, o, nx, plane, o));
+    }
+    return HH_OK;
+}
+
+// -------------------------------------------------------------------- plans ------
+static int plan_alloc(hh_plan *pl) {
+    Plan &p = pl->p;
+    HH_CUDA(cudaMalloc(&p.Lf, sizeof(double2) * (size_t)p.lines * p.rows));
+    HH_CUDA(cudaMalloc(&p.Ui, sizeof(double2) * (size_t)p.lines * p.rows));
+    HH_CUDA(cudaMalloc(&p.rowc, sizeof(double2) * 4 * (size_t)p.rows));
+    HH_CUDA(cudaMalloc(&p.mu, sizeof(double) * 3 * (size_t)p.lines));
+    return HH_OK;
+}
+
+static void plan_free(hh_plan *pl) {
+    Plan &p = pl->p;
+    cudaFree(p.Lf);
+    cudaFree(p.Ui);
+    cudaFree(p.rowc);
+    cudaFree(p.mu);
+    cudaFree(p.pade_l);
+    cudaFree(p.pade_u);
+    cudaFree(pl->stage);
+}
+
+// [1 10 1] Pade factors along the line direction (the reference's constant-coefficient solves,
+// 2D_Program/partial_derivatives/4th_order_second_derivative.c:19-24,
+// 3D_Program/partial_derivatives/4th_order_partials.c:118-123): U_0 = 10, L_r = 1/U_{r-1},
+// U_r = 10 - L_r; the device keeps L_r (L_0 = 0) and 1/U_r.
+static int plan_pade(hh_plan *pl) {
+    Plan &p = pl->p;
+    std::vector<double> L(p.rows), Ui(p.rows);
+    double U = 10.0;
+    L[0] = 0.0;
+    Ui[0] = 1.0 / U;
+    for (int r = 1; r < p.rows; r++) {
+        L[r] = 1.0 / U;
+        U = 10.0 - L[r];
+        Ui[r] = 1.0 / U;
+    }
+    HH_CUDA(cudaMalloc(&p.pade_l, sizeof(double) * (size_t)p.rows));
+    HH_CUDA(cudaMalloc(&p.pade_u, sizeof(double) * (size_t)p.rows));
+    HH_CUDA(cudaMemcpy(p.pade_l, L.data(), sizeof(double) * (size_t)p.rows, cudaMemcpyHostToDevice));
+    HH_CUDA(cudaMemcpy(p.pade_u, Ui.data(), sizeof(double) * (size_t)p.rows, cudaMemcpyHostToDevice));
+    return HH_OK;
+}
+
+// Build factors from host tables: sub/diag/sup are 4*rows complex each (see hh_tridiag.cu).
+static int plan_factor(hh_plan *pl, const std::vector<double2> &sub, const std::vector<double2> &dia,
+                       const std::vector<double2> &sup, const std::vector<double> &mu) {
+    Plan &p = pl->p;
+    Ctx  *c = p.ctx;
+    double2 *dsub = nullptr, *ddia = nullptr;
+    const size_t tb = sizeof(double2) * 4 * (size_t)p.rows;
+    HH_CUDA(cudaMalloc(&dsub, tb));
+    HH_CUDA(cudaMalloc(&ddia, tb));
+    int rc = upload(c, dsub, sub.data(), tb);
+    if (rc == HH_OK) rc = upload(c, ddia, dia.data(), tb);
+    if (rc == HH_OK) rc = upload(c, p.rowc, sup.data(), tb);
+    if (rc == HH_OK) rc = upload(c, p.mu, mu.data(), sizeof(double) * 3 * (size_t)p.lines);
+    if (rc == HH_OK) rc = launch_factor(&p, dsub, ddia, p.rowc);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    cudaFree(dsub);
+    cudaFree(ddia);
+    if (rc != HH_OK) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "factorisation", __FILE__, __LINE__);
+    return HH_OK;
+}
+
+static inline double2 cget(const double *a, int j) { return make_double2(a[2 * j], a[2 * j + 1]); }
+
+extern "C" int hh_plan2d_create(hh_ctx *x, int nx, int ny, const double *bp, const double *ap, const double *b,
+                                const double *a, const double *bm, const double *am, hh_plan **out) {
+    if (!x || !out || nx < 1 || ny < 1 || !bp || !ap || !b || !a || !bm || !am) {
+        set_error("hh_plan2d_create: invalid arguments");
+        return HH_ERR_INVALID;
+    }
+    *out = nullptr;
+    HH_CUDA(cudaSetDevice(x->c.device));
+    hh_plan *pl = new hh_plan();
+    Plan    &p = pl->p;
+    p.ctx = &x->c;
+    p.dim = 2;
+    p.nx = nx;
+    p.ny = ny;
+    p.lines = nx;
+    p.rows = ny;
+    p.row_stride = nx;
+    p.field = (long)nx * ny;
+    int rc = plan_alloc(pl);
+    if (rc != HH_OK) { plan_free(pl); delete pl; return rc; }
+    // eigenvalues of the x second difference, as 2D LU.c:12-14
+    std::vector<double> mu(3 * (size_t)nx, 0.0);
+    for (int i = 0; i < nx; i++) mu[nx + i] = 2.0 * cos((i + 1) * M_PI / (nx + 1));
+    std::vector<double2> sub(4 * (size_t)ny), dia(4 * (size_t)ny), sup(4 * (size_t)ny);
+    const double2 z = make_double2(0.0, 0.0);
+    for (int j = 0; j < ny; j++) {
+        sub[j] = z; sub[ny + j] = cget(bm, j); sub[2 * ny + j] = z; sub[3 * ny + j] = cget(am, j);
+        dia[j] = z; dia[ny + j] = cget(b, j);  dia[2 * ny + j] = z; dia[3 * ny + j] = cget(a, j);
+        sup[j] = z; sup[ny + j] = cget(bp, j); sup[2 * ny + j] = z; sup[3 * ny + j] = cget(ap, j);
+    }
+    rc = plan_factor(pl, sub, dia, sup, mu);
+    if (rc != HH_OK) { plan_free(pl); delete pl; return rc; }
+    *out = pl;
+    return HH_OK;
+}
+
+extern "C" int hh_plan3d_create(hh_ctx *x, int nx, int ny, int nz, const double *const coef[12], hh_plan **out) {
+    if (!x || !out || nx < 1 || ny < 1 || nz < 1 || !coef) {
+        set_error("hh_plan3d_create: invalid arguments");
+        return HH_ERR_INVALID;
+    }
+    for (int t = 0; t < 12; t++)
+        if (!coef[t]) { set_error("hh_plan3d_create: null coefficient %d", t); return HH_ERR_INVALID; }
+    *out = nullptr;
+    HH_CUDA(cudaSetDevice(x->c.device));
+    hh_plan *pl = new hh_plan();
+    Plan    &p = pl->p;
+    p.ctx = &x->c;
+    p.dim = 3;
+    p.nx = nx;
+    p.ny = ny;
+    p.nz = nz;
+    p.lines = nx * ny;
+    p.rows = nz;
+    p.row_stride = (long)nx * ny;
+    p.field = (long)nx * ny * nz;
+    int rc = plan_alloc(pl);
+    if (rc != HH_OK) { plan_free(pl); delete pl; return rc; }
+    // eigenvalue products per (i,j) line, as 3D LU.c:31-44
+    std::vector<double> mu(3 * (size_t)p.lines);
+    for (int j = 0; j < ny; j++) {
+        const double ey = 2.0 * cos((j + 1) * M_PI / (ny + 1));
+        for (int i = 0; i < nx; i++) {
+            const double ex = 2.0 * cos((i + 1) * M_PI / (nx + 1));
+            const long   q = i + (long)j * nx;
+            mu[q] = ex * ey;
+            mu[p.lines + q] = ex;
+            mu[2 * (size_t)p.lines + q] = ey;
+        }
+    }
+    // coef order a,b,c,d,ap,bp,cp,dp,am,bm,cm,dm -> (corner, x-neighbour, y-neighbour, centre)
+    std::vector<double2> sub(4 * (size_t)nz), dia(4 * (size_t)nz), sup(4 * (size_t)nz);
+    for (int l = 0; l < nz; l++)
+        for (int t = 0; t < 4; t++) {
+            dia[t * (size_t)nz + l] = cget(coef[t], l);
+            sup[t * (size_t)nz + l] = cget(coef[4 + t], l);
+            sub[t * (size_t)nz + l] = cget(coef[8 + t], l);
+        }
+    rc = plan_factor(pl, sub, dia, sup, mu);
+    if (rc != HH_OK) { plan_free(pl); delete pl; return rc; }
+    *out = pl;
+    return HH_OK;
+}
+
+extern "C" int hh_plan2d_create_helmholtz(hh_ctx *x, int n, int order, double kr, double ki, hh_plan **out) {
+    std::vector<double> buf(6 * 2 * (size_t)n);
+    double *arr[6];
+    for (int t = 0; t < 6; t++) arr[t] = buf.data() + t * 2 * (size_t)n;
+    int rc = hh_coefficients2d(n, order, kr, ki, arr);
+    if (rc != HH_OK) { set_error("hh_plan2d_create_helmholtz: order must be 2, 4 or 6"); return rc; }
+    HH_TRY(hh_plan2d_create(x, n, n, arr[0], arr[1], arr[2], arr[3], arr[4], arr[5], out));
+    Plan &p = (*out)->p;
+    p.order = order;
+    p.src_order = order;
+    p.h = 1.0 / (n + 1);
+    p.k2 = make_double2(kr * kr - ki * ki, 2.0 * kr * ki);
+    int rc2 = plan_pade(*out);
+    if (rc2 != HH_OK) { hh_plan_destroy(*out); *out = nullptr; return rc2; }
+    return HH_OK;
+}
+
+extern "C" int hh_plan3d_create_helmholtz(hh_ctx *x, int n, int order, double kr, double ki, hh_plan **out) {
+    std::vector<double> buf(12 * 2 * (size_t)n);
+    double *arr[12];
+    for (int t = 0; t < 12; t++) arr[t] = buf.data() + t * 2 * (size_t)n;
+    int rc = hh_coefficients3d(n, order, kr, ki, arr);
+    if (rc != HH_OK) { set_error("hh_plan3d_create_helmholtz: order must be 2, 4 or 6"); return rc; }
+    const double *carr[12];
+    for (int t = 0; t < 12; t++) carr[t] = arr[t];
+    HH_TRY(hh_plan3d_create(x, n, n, n, carr, out));
+    Plan &p = (*out)->p;
+    p.order = order;
+    p.src_order = order;
+    p.h = 1.0 / (n + 1);
+    p.k2 = make_double2(kr * kr - ki * ki, 2.0 * kr * ki);
+    int rc2 = plan_pade(*out);
+    if (rc2 != HH_OK) { hh_plan_destroy(*out); *out = nullptr; return rc2; }
+    return HH_OK;
+}
+
+extern "C" int hh_plan_destroy(hh_plan *pl) {
+    if (!pl) return HH_OK;
+    cudaSetDevice(pl->p.ctx->device);
+    cudaStreamSynchronize(pl->p.ctx->stream);
+    plan_free(pl);
+    delete pl;
+    return HH_OK;
+}
+
+extern "C" long hh_plan_field_size(const hh_plan *pl) { return pl ? pl->p.field : 0; }
+
+// -------------------------------------------------------------------- solve ------
+static int transform_forward(Plan &p, const double2 *in, double2 *out, int batch) {
+    Ctx *c = p.ctx;
+    if (p.dim == 2) return launch_dst_rows(c, p.nx, (long)p.ny * batch, in, p.nx, out, p.nx);
+    const long plane = (long)p.nx * p.ny, planes = (long)p.nz * batch;
+    HH_TRY(launch_dst_rows(c, p.nx, (long)p.ny * planes, in, p.nx, out, p.nx));
+    for (long p0 = 0; p0 < planes; p0 += 65535) {
+        const long np = (planes - p0 < 65535) ? planes - p0 : 65535;
+        HH_TRY(launch_dst_cols(c, p.ny, p.nx, np, out + p0 * plane, p.nx, plane, out + p0 * plane));
+    }
+    return HH_OK;
+}
+
+static int transform_inverse(Plan &p, double2 *buf, int batch) {
+    Ctx *c = p.ctx;
+    if (p.dim == 2) return launch_dst_rows(c, p.nx, (long)p.ny * batch, buf, p.nx, buf, p.nx);
+    const long plane = (long)p.nx * p.ny, planes = (long)p.nz * batch;
+    for (long p0 = 0; p0 < planes; p0 += 65535) {
+        const long np = (planes - p0 < 65535) ? planes - p0 : 65535;
+        HH_TRY(launch_dst_cols(c, p.ny, p.nx, np, buf + p0 * plane, p.nx, plane, buf + p0 * plane));
+    }
+    return launch_dst_rows(c, p.nx, (long)p.ny * planes, buf, p.nx, buf, p.nx);
+}
+
+static int check_batch(hh_plan *pl, int batch) {
+    if (!pl || batch < 0 || batch > 65535) {
+        set_error("invalid plan or batch (%d)", batch);
+        return HH_ERR_INVALID;
+    }
+    return HH_OK;
+}
+
+extern "C" int hh_solve(hh_plan *pl, const double *rhs, double *sol, int batch) {
+    HH_TRY(check_batch(pl, batch));
+    if (batch == 0) return HH_OK;
+    if (!rhs || !sol) { set_error("hh_solve: null buffer"); return HH_ERR_INVALID; }
+    Plan &p = pl->p;
+    HH_CUDA(cudaSetDevice(p.ctx->device));
+    double2 *u = (double2 *)sol;
+    HH_TRY(stage_mark(*p.ctx, 0));
+    HH_TRY(transform_forward(p, (const double2 *)rhs, u, batch));
+    HH_TRY(stage_mark(*p.ctx, 1));
+    HH_TRY(launch_line_solve(&p, u, u, batch, 0));
+    HH_TRY(stage_mark(*p.ctx, 2));
+    HH_TRY(transform_inverse(p, u, batch));
+    return stage_mark(*p.ctx, 3);
+}
+
+extern "C" int hh_solve_source(hh_plan *pl, const double *f, double *u, int batch) {
+    HH_TRY(check_batch(pl, batch));
+    if (batch == 0) return HH_OK;
+    if (!f || !u) { set_error("hh_solve_source: null buffer"); return HH_ERR_INVALID; }
+    Plan &p = pl->p;
+    if (p.src_order == 0) {
+        set_error("hh_solve_source needs a plan from hh_plan{2,3}d_create_helmholtz");
+        return HH_ERR_INVALID;
+    }
+    HH_CUDA(cudaSetDevice(p.ctx->device));
+    double2 *w = (double2 *)u;
+    HH_TRY(stage_mark(*p.ctx, 0));
+    HH_TRY(transform_forward(p, (const double2 *)f, w, batch));
+    HH_TRY(stage_mark(*p.ctx, 1));
+    HH_TRY(launch_line_solve(&p, w, w, batch, p.src_order));
+    HH_TRY(stage_mark(*p.ctx, 2));
+    HH_TRY(transform_inverse(p, w, batch));
+    return stage_mark(*p.ctx, 3);
+}
+
+static int solve_host_common(hh_plan *pl, const double *in_host, double *out_host, int batch, bool source) {
+    HH_TRY(check_batch(pl, batch));
+    if (batch == 0) return HH_OK;
+    if (!in_host || !out_host) { set_error("host solve: null buffer"); return HH_ERR_INVALID; }
+    Plan &p = pl->p;
+    Ctx  *c = p.ctx;
+    HH_CUDA(cudaSetDevice(c->device));
+    const long need = p.field * batch;
+    if (pl->stage_elems < need) {
+        cudaFree(pl->stage);
+        pl->stage = nullptr;
+        pl->stage_elems = 0;
+        HH_CUDA(cudaMalloc(&pl->stage, sizeof(double2) * (size_t)need));
+        pl->stage_elems = need;
+    }
+    const size_t bytes = sizeof(double2) * (size_t)need;
+    HH_CUDA(cudaMemcpyAsync(pl->stage, in_host, bytes, cudaMemcpyHostToDevice, c->stream));
+    const double *d = (const double *)pl->stage;
+    HH_TRY(source ? hh_solve_source(pl, d, (double *)pl->stage, batch) : hh_solve(pl, d, (double *)pl->stage, batch));
+    HH_CUDA(cudaMemcpyAsync(out_host, pl->stage, bytes, cudaMemcpyDeviceToHost, c->stream));
+    hh_ctx *owner = reinterpret_cast<hh_ctx *>(c); // Ctx is the first member of hh_ctx
+    return hh_ctx_synchronize(owner);
+}
+
+extern "C" int hh_solve_host(hh_plan *pl, const double *rhs, double *sol, int batch) {
+    return solve_host_common(pl, rhs, sol, batch, false);
+}
+extern "C" int hh_solve_source_host(hh_plan *pl, const double *f, double *u, int batch) {
+    return solve_host_common(pl, f, u, batch, true);
+}

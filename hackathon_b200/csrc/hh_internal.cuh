@@ -1,0 +1,118 @@
+// Internal declarations shared by the sm_100a kernels and the C-ABI layer.
+//
+// Data layout: complex double stored as interleaved (re, im) double2, x fastest, exactly as
+// the reference's `double _Complex` arrays (2D_Program/headers/structs.h:9,
+// 3D_Program/headers/structs.h:36) so host buffers cross the boundary without repacking.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/hh.h"
+
+namespace hh {
+
+// ------------------------------------------------------------------ errors ------
+void set_error(const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line);
+
+#define HH_CUDA(call)                                                                  \
+    do {                                                                               \
+        cudaError_t hh_e_ = (call);                                                    \
+        if (hh_e_ != cudaSuccess) return ::hh::cuda_fail(hh_e_, #call, __FILE__, __LINE__); \
+    } while (0)
+
+#define HH_TRY(call)                        \
+    do {                                    \
+        int hh_rc_ = (call);                \
+        if (hh_rc_ != HH_OK) return hh_rc_; \
+    } while (0)
+
+// ------------------------------------------------------------ complex math ------
+__host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+// a - b*c
+__host__ __device__ __forceinline__ double2 cfms(double2 a, double2 b, double2 c) {
+    return make_double2(a.x - (b.x * c.x - b.y * c.y), a.y - (b.x * c.y + b.y * c.x));
+}
+// a + b*c
+__host__ __device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {
+    return make_double2(a.x + (b.x * c.x - b.y * c.y), a.y + (b.x * c.y + b.y * c.x));
+}
+// 1/z by the textbook formula conj(z)/|z|^2 (inputs are O(1) Thomas pivots)
+__host__ __device__ __forceinline__ double2 crcp(double2 z) {
+    double d = 1.0 / (z.x * z.x + z.y * z.y);
+    return make_double2(z.x * d, -z.y * d);
+}
+__host__ __device__ __forceinline__ double2 cdiv(double2 a, double2 b) { return cmul(a, crcp(b)); }
+
+// ---------------------------------------------------------------- context -------
+struct Plan;
+
+struct Ctx {
+    int          device = 0;
+    cudaStream_t stream = nullptr;
+    bool         own_stream = false;
+    // device twiddle tables keyed by transform length M (= n + 1):
+    //   tw[M]  : exp(-2 pi i t / M), t = 0..M-1                 (double2)
+    //   sn[M]  : sin(pi t / M),      t = 0..M-1                 (double)
+    std::map<int, double2 *> tw;
+    std::map<int, double *>  sn;
+    std::map<int, double *>  dense; // n*n sine matrices for the direct DST (n+1 not a power of two)
+    std::mutex               mu;
+    std::vector<Plan *>      plans;
+    long long                launches = 0;       // kernels launched through this context
+    int                     *err_word = nullptr; // set by kernels whose bounded waits expire
+    // stage timing (hh_ctx_set_stage_timing)
+    bool                     timing = false;
+    std::vector<cudaEvent_t> ev_pending;          // groups of 4 events per timed solve
+    double                   stage_ms[3] = {0, 0, 0};
+    long long                timed_solves = 0;
+};
+
+int tables_for(Ctx *c, int m, const double2 **tw, const double **sn);
+int dense_for(Ctx *c, int n, const double **mat);
+
+// Plan: one (dim, sizes, stencil coefficients) problem with its device-resident setup.
+struct Plan {
+    Ctx   *ctx = nullptr;
+    int    dim = 2;
+    int    nx = 0, ny = 0, nz = 1;
+    int    order = 6;
+    // line-solve geometry: `lines` independent lines of `rows` points; element (row r, line q)
+    // at offset r*row_stride + q inside one right-hand side.
+    int    lines = 0, rows = 0;
+    long   row_stride = 0;
+    long   field = 0;               // complex elements per right-hand side
+    // factors in [row][line] layout (line fastest): Lf = sub-diagonal multiplier, Ui = 1/pivot
+    double2 *Lf = nullptr, *Ui = nullptr;
+    // super-diagonal Up(row, line) = sum_t rowc[t][row] * mu[t][line] + rowc[3][row]
+    double2 *rowc = nullptr;        // 4 * rows complex
+    double  *mu = nullptr;          // 3 * lines real
+    double2 *scratch = nullptr;     // one field per batch slot (transformed data)
+    int      scratch_batch = 0;
+    // fused source operator (homogeneous Dirichlet, constant k): 0 = off
+    int      src_order = 0;
+    double  *pade_l = nullptr, *pade_u = nullptr; // [1 10 1] factors along the line (rows each)
+    double   h = 0.0;
+    double2  k2 = {0.0, 0.0};
+};
+
+int launch_dst_rows(Ctx *c, int n, long rows, const double2 *in, long in_ld, double2 *out, long out_ld);
+int launch_dst_cols(Ctx *c, int n, long ncols, long planes, const double2 *in, long ld, long plane_stride,
+                    double2 *out);
+int launch_factor(Plan *p, const double2 *subt, const double2 *diagt, const double2 *supt);
+int launch_line_solve(Plan *p, const double2 *in, double2 *out, int batch, int src_order);
+int read_device_error(Ctx *c, int *val);
+
+} // namespace hh

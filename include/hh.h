@@ -1,0 +1,128 @@
+/*
+ * hh.h -- C ABI of the B200 (sm_100a) compact Helmholtz direct solver.
+ *
+ * The solver follows gonzrona/hackathon: orthonormal DST-I in the constant-coefficient
+ * direction(s), shifted tridiagonal line solves in the remaining direction, inverse DST-I
+ * (2D_Program/solver_functions/solver.c:14-117, 3D_Program/solver_functions/solver.c:390-540).
+ *
+ * Conventions
+ *  - Complex values are C99 `double _Complex` / interleaved (re, im) doubles; a `const double *`
+ *    argument that carries complex data points at 2*count doubles.
+ *  - Fields are x fastest: 2D index i + j*nx, 3D index i + j*nx + l*nx*ny (as the reference,
+ *    2D_Program/headers/structs.h:9).  A batch of fields is contiguous, field after field.
+ *  - Every function returns an int status (HH_OK = 0); hh_last_error() returns a message for the
+ *    calling thread's most recent failure.  The reference's own entry points return void and
+ *    print CUDA errors (solver_functions/cuda_helper.h:33-48); the drop-in libraries keep that
+ *    signature (hh_dropin2d.h, hh_dropin3d.h) and report through hh_last_error().
+ *  - "_dev" pointers are device memory on the context's device; "_host" pointers are host memory.
+ *  - One context = one device + one CUDA stream; a context is used by one host thread at a
+ *    time.  Separate contexts are independent.
+ *  - Failures never fall back to a CPU path: if the CUDA module cannot run, calls fail.
+ */
+#ifndef HH_H
+#define HH_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HH_OK              0
+#define HH_ERR_INVALID     1  /* bad argument                                   */
+#define HH_ERR_CUDA        2  /* CUDA runtime error                             */
+#define HH_ERR_NOMEM       3  /* device allocation failed                       */
+#define HH_ERR_UNSUPPORTED 4  /* size or option not implemented                 */
+#define HH_ERR_DEVICE      5  /* a kernel reported a failure (bounded wait hit) */
+
+typedef struct hh_ctx  hh_ctx;
+typedef struct hh_plan hh_plan;
+
+/* ---------------------------------------------------------------- library ---- */
+const char *hh_last_error(void);
+int         hh_version(void);                 /* major*10000 + minor*100 + patch */
+
+/* --------------------------------------------------------------- contexts ---- */
+/* stream: a cudaStream_t to launch on, or NULL for a context-owned stream. */
+int hh_ctx_create(int device, void *stream, hh_ctx **out);
+int hh_ctx_destroy(hh_ctx *ctx);
+int hh_ctx_set_stream(hh_ctx *ctx, void *stream);
+int hh_ctx_synchronize(hh_ctx *ctx);          /* also surfaces kernel-reported failures   */
+long long hh_ctx_launch_count(const hh_ctx *ctx); /* kernels launched through this context */
+
+/* Stage timing: when enabled, every solve records CUDA events on the context's stream around
+ * its three stages (forward transform, line solves, inverse transform) and accumulates the
+ * elapsed device time.  hh_ctx_stage_times() synchronizes, then returns per-stage totals in
+ * milliseconds and the number of solves timed, and resets them. */
+#define HH_STAGE_FORWARD 0
+#define HH_STAGE_LINES   1
+#define HH_STAGE_INVERSE 2
+#define HH_NUM_STAGES    3
+int hh_ctx_set_stage_timing(hh_ctx *ctx, int on);
+int hh_ctx_stage_times(hh_ctx *ctx, double ms[HH_NUM_STAGES], long long *solves);
+
+/* device memory helpers for callers without their own CUDA bindings */
+int hh_malloc(hh_ctx *ctx, size_t bytes, void **ptr_dev);
+int hh_free(hh_ctx *ctx, void *ptr_dev);
+int hh_memcpy_h2d(hh_ctx *ctx, void *dst_dev, const void *src_host, size_t bytes);
+int hh_memcpy_d2h(hh_ctx *ctx, void *dst_host, const void *src_dev, size_t bytes);
+
+/* ------------------------------------------------------------- transforms ---- */
+/* Orthonormal DST-I of `rows` contiguous complex rows of length n (row r at offset r*ld).
+ * Replaces forwardDST/reverseDST, 2D_Program/solver_functions/DST.c:6,26, which take the
+ * same transform of every row through two zero-padded length-(2n+2) real FFTs. */
+int hh_dst1_rows(hh_ctx *ctx, int n, long rows, const double *in_dev, long in_ld, double *out_dev, long out_ld);
+
+/* DST-I along the strided direction: for each of `planes` planes (plane stride
+ * plane_stride), transform each of `ncols` columns whose element j sits at col + j*ld. */
+int hh_dst1_cols(hh_ctx *ctx, int n, long ncols, long planes, const double *in_dev, long ld, long plane_stride,
+                 double *out_dev);
+
+/* 2D DST-I (x then y) of nz planes of nx*ny complex values, in place or out of place.
+ * Replaces DST(), 3D_Program/solver_functions/DST.c:148 (one real plane through two FFTW
+ * batches and a transpose) and DST1/DST2 (DST.c:13,50). */
+int hh_dst2_planes(hh_ctx *ctx, int nx, int ny, long nplanes, const double *in_dev, double *out_dev);
+
+/* ------------------------------------------------------------------ plans ---- */
+/* 2D plan from the reference's per-row 9-point stencil [bm am bm; b a b; bp ap bp]
+ * (2D_Program/main_functions/coefficients.c:5-7), each array ny complex values on the host.
+ * Builds the shifted Thomas factors on the device (replaces LU(), 2D_Program/main_functions/LU.c:3). */
+int hh_plan2d_create(hh_ctx *ctx, int nx, int ny, const double *bp, const double *ap, const double *b,
+                     const double *a, const double *bm, const double *am, hh_plan **out);
+
+/* 3D plan from the reference's per-layer 27-point stencil a..dm (3D_Program/main_functions/
+ * coefficients.c, order a,b,c,d,ap,bp,cp,dp,am,bm,cm,dm), each nz complex values on the host.
+ * Replaces LU(), 3D_Program/main_functions/LU.c:4. */
+int hh_plan3d_create(hh_ctx *ctx, int nx, int ny, int nz, const double *const coef[12], hh_plan **out);
+
+/* Plans for the constant-k, unit-domain, homogeneous-Dirichlet problem class with the compact
+ * right-hand-side operator fused into the line solve (order 2, 4 or 6).  The stencil follows
+ * coefficients.c (2D :9-61, 3D :293-389) with k constant. */
+int hh_plan2d_create_helmholtz(hh_ctx *ctx, int n, int order, double k_re, double k_im, hh_plan **out);
+int hh_plan3d_create_helmholtz(hh_ctx *ctx, int n, int order, double k_re, double k_im, hh_plan **out);
+
+int hh_plan_destroy(hh_plan *plan);
+long hh_plan_field_size(const hh_plan *plan);  /* complex values per right-hand side */
+
+/* Solve A u = rhs for `batch` assembled right-hand sides (the reference's solver(System),
+ * 2D_Program/solver_functions/solver.c:14, 3D_Program/solver_functions/solver.c:390). */
+int hh_solve(hh_plan *plan, const double *rhs_dev, double *sol_dev, int batch);
+/* Same with host buffers: host-to-device copy, solve, device-to-host copy on the plan's stream. */
+int hh_solve_host(hh_plan *plan, const double *rhs_host, double *sol_host, int batch);
+
+/* Helmholtz plans only: u from the source samples f at the interior grid points (the
+ * compact right-hand side is assembled on the device; replaces rhs(),
+ * 2D_Program/main_functions/rhs.c:100, 3D_Program/main_functions/rhs.c:198, for this class). */
+int hh_solve_source(hh_plan *plan, const double *f_dev, double *u_dev, int batch);
+int hh_solve_source_host(hh_plan *plan, const double *f_host, double *u_host, int batch);
+
+/* Stencil coefficients the Helmholtz plans use (host arrays of n complex values each):
+ * 2D order in bp,ap,b,a,bm,am order; 3D in a..dm order (12 arrays). */
+int hh_coefficients2d(int n, int order, double k_re, double k_im, double *const out[6]);
+int hh_coefficients3d(int n, int order, double k_re, double k_im, double *const out[12]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HH_H */

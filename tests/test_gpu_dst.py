@@ -1,0 +1,87 @@
+"""GPU parity of the DST-I kernels against the oracle (and the reference's golden rows)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+from conftest import golden, rel_err
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+SIZES = [1, 2, 7, 63, 100, 127, 255, 300, 511, 1023, 2047, 4095, 8191]
+
+
+def _dev(a: np.ndarray):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _host(t) -> np.ndarray:
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+@pytest.mark.parametrize("n", SIZES)
+def test_dst_rows_matches_oracle(ctx, oracle, n):
+    rows = 37 if n < 4000 else 5
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal((rows, n)) + 1j * rng.standard_normal((rows, n))
+    src, dst = _dev(x), torch.empty((rows, n), dtype=torch.complex128, device="cuda")
+    ctx.dst1_rows(n, rows, src, dst)
+    ctx.synchronize()
+    assert rel_err(_host(dst), oracle.dst1_rows(x)) < 1e-13
+
+
+def test_dst_rows_golden_and_in_place(ctx):
+    g = golden("dst_rows.npz")
+    for n in (1, 7, 31, 63, 100):
+        t = _dev(g[f"x_{n}"])
+        ctx.dst1_rows(n, t.shape[0], t, t)  # in place
+        ctx.synchronize()
+        assert rel_err(_host(t), g[f"y_{n}"]) < 1e-13
+
+
+def test_dst_is_an_involution(ctx):
+    n, rows = 1023, 64
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((rows, n)) + 1j * rng.standard_normal((rows, n))
+    t = _dev(x)
+    ctx.dst1_rows(n, rows, t, t)
+    ctx.dst1_rows(n, rows, t, t)
+    ctx.synchronize()
+    assert rel_err(_host(t), x) < 1e-13
+
+
+@pytest.mark.parametrize("n,ncols,planes", [(255, 255, 3), (63, 100, 2), (100, 37, 2), (1023, 64, 1), (7, 5, 4)])
+def test_dst_cols_matches_oracle(ctx, oracle, n, ncols, planes):
+    rng = np.random.default_rng(n + ncols)
+    x = rng.standard_normal((planes, n, ncols)) + 1j * rng.standard_normal((planes, n, ncols))
+    t = _dev(x)
+    ctx.dst1_cols(n, ncols, planes, t, ncols, n * ncols, t)
+    ctx.synchronize()
+    ref = np.stack([oracle.dst1_rows(np.ascontiguousarray(x[p].T)).T for p in range(planes)])
+    assert rel_err(_host(t), ref) < 1e-13
+
+
+@pytest.mark.parametrize("nx,ny", [(255, 255), (31, 63), (100, 15)])
+def test_dst2_planes_matches_reference_plane_transform(ctx, oracle, nx, ny):
+    """hh_dst2_planes against the reference's 3D DST() restated (3D DST.c:148-204) on the real
+    and imaginary planes."""
+    planes = 3
+    rng = np.random.default_rng(nx * ny)
+    x = rng.standard_normal((planes, ny, nx)) + 1j * rng.standard_normal((planes, ny, nx))
+    t = _dev(x)
+    ctx.dst2_planes(nx, ny, planes, t, t)
+    ctx.synchronize()
+    ref = np.empty_like(x)
+    for p in range(planes):
+        for part, put in ((x[p].real, 1.0), (x[p].imag, 1j)):
+            inp = np.ascontiguousarray(part)
+            out = np.zeros_like(inp)
+            oracle.lib.ora_dst2_plane_real(C.c_int(nx), C.c_int(ny), inp.ctypes.data_as(C.POINTER(C.c_double)),
+                                           out.ctypes.data_as(C.POINTER(C.c_double)))
+            if put == 1.0:
+                ref[p] = out
+            else:
+                ref[p] += 1j * out
+    assert rel_err(_host(t), ref) < 1e-13

@@ -1,0 +1,99 @@
+"""GPU parity of the full solve (plain FP64) against the oracle restatement, which is itself
+bit-exact with the reference's C code (tests/test_oracle.py)."""
+import numpy as np
+import pytest
+from conftest import golden, rel_err
+
+import hackathon_b200 as hh
+from hackathon_b200 import workload as W
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12  # plain FP64 form vs the reference path: max|u - u_ref| / max|u_ref|
+
+
+def _source(n, seed, pmax=20, noise=1e-3):
+    return W.source_2d(n, W.sine_modes(seed, 8, pmax), noise_seed=seed + 1 if noise else None, noise_var=noise)
+
+
+@pytest.mark.parametrize("n,order,k", [(15, 6, 10.0), (16, 4, 50.0), (31, 2, 10.0), (63, 6, 200.0), (100, 6, 10.0),
+                                       (127, 4, 50.0), (255, 6, 50.0), (300, 6, 20.0), (511, 2, 30.0),
+                                       (1023, 6, 10.0), (1023, 4, 200.0)])
+def test_solver2d_assembled_rhs_matches_oracle(ctx, oracle, n, order, k):
+    """drop-in path: solver() on the reference's assembled rhs with its coefficient rows."""
+    f = _source(n, n + order)
+    ref = oracle.pipeline_2d(n, order, k, f)
+    plan = hh.Plan.from_coefficients_2d(ctx, n, n, ref["coef"])
+    sol = plan.solve_host(ref["rhs"])
+    assert rel_err(sol, ref["sol"]) < TOL
+    plan.close()
+
+
+@pytest.mark.parametrize("n,order,k", [(15, 6, 10.0), (31, 4, 50.0), (31, 2, 10.0), (100, 6, 10.0), (255, 6, 50.0),
+                                       (1023, 6, 50.0), (1023, 4, 10.0), (1023, 6, 200.0), (2047, 6, 100.0)])
+def test_solver2d_fused_source_matches_oracle(ctx, oracle, n, order, k):
+    """Helmholtz plan: RHS assembly fused on the device vs the reference pipeline
+    coefficients -> rhs -> LU -> solver."""
+    f = _source(n, 3 * n + order)
+    ref = oracle.pipeline_2d(n, order, k, f)
+    plan = hh.Plan.helmholtz(ctx, 2, n, order, k)
+    u = plan.solve_source_host(f[1:-1, 1:-1])
+    assert rel_err(u, ref["sol"]) < TOL
+    plan.close()
+
+
+def test_readme_case_against_golden_and_exact(ctx):
+    """./Direct_Solver 6 100 class: the reference's own output (golden) and the manufactured
+    exact solution."""
+    g = golden("ref2d_o6_n100_k10_readme.npz")
+    n = int(g["n"])
+    m = W.sine_modes(int(g["seed"]), 8, int(g["pmax"]))
+    f = W.source_2d(n, m)
+    plan = hh.Plan.helmholtz(ctx, 2, n, 6, 10.0)
+    u = plan.solve_source_host(f[1:-1, 1:-1])
+    assert rel_err(u, g["sol"]) < TOL
+    exact = W.exact_2d(n, m, 10.0)
+    # 6th-order discretisation error at h = 1/101 with modes up to p = 20: (20 pi h)^6 / 6! scale
+    assert rel_err(u, exact) < 1e-5
+
+
+def test_batch_equals_single(ctx, oracle):
+    n, order, k, B = 255, 6, 50.0, 6
+    fs = np.stack([_source(n, 100 + b)[1:-1, 1:-1] for b in range(B)])
+    plan = hh.Plan.helmholtz(ctx, 2, n, order, k)
+    ub = plan.solve_source_host(fs)
+    for b in (0, 3, 5):
+        assert np.array_equal(plan.solve_source_host(fs[b]), ub[b])  # bitwise: alone == in batch
+
+
+@pytest.mark.parametrize("n,order,k", [(15, 6, 30.0), (31, 6, 30.0), (31, 4, 10.0), (63, 2, 20.0), (127, 6, 30.0)])
+def test_solver3d_fused_source_matches_oracle(ctx, oracle, n, order, k):
+    m = W.sine_modes(n + order, 16, min(n, 64), dim=3)
+    f = W.source_3d(n, m)
+    ref = oracle.pipeline_3d(n, order, k, f)
+    plan = hh.Plan.helmholtz(ctx, 3, n, order, k)
+    u = plan.solve_source_host(f[1:-1, 1:-1, 1:-1])
+    assert rel_err(u, ref["sol"]) < TOL
+    # drop-in path on the assembled rhs
+    plan3 = hh.Plan.from_coefficients_3d(ctx, n, n, n, ref["coef"])
+    assert rel_err(plan3.solve_host(ref["rhs"]), ref["sol"]) < TOL
+
+
+@pytest.mark.parametrize("name", ["paper_o6_n11", "paper_o4_n11", "default_o6_n13"])
+def test_solver3d_reference_problem_golden(ctx, name):
+    """The reference's own 3D problems (variable k(z) for the paper case): our solver on the
+    reference's assembled rhs and per-layer stencil vs its own solve."""
+    g = golden(f"ref3d_{name}.npz")
+    n = int(g["n"])
+    coef = {nm: g[f"c_{nm}"] for nm in ("a", "b", "c", "d", "ap", "bp", "cp", "dp", "am", "bm", "cm", "dm")}
+    plan = hh.Plan.from_coefficients_3d(ctx, n, n, n, coef)
+    assert rel_err(plan.solve_host(g["rhs"]), g["sol"]) < TOL
+
+
+def test_invalid_arguments(ctx):
+    with pytest.raises(hh.HHError):
+        hh.Plan.helmholtz(ctx, 2, 31, 5, 10.0)
+    plan = hh.Plan.helmholtz(ctx, 2, 31, 6, 10.0)
+    with pytest.raises(hh.HHError):
+        plan.solve(0, 0, 1)
+    plan.solve(0, 0, 0)  # empty batch is a no-op
