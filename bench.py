@@ -168,8 +168,8 @@ def run_reference(args, rank: int) -> None:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=12)
-    ap.add_argument("--warmup", type=int, default=6)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -188,18 +188,19 @@ def main():
 
     import hackathon_b200 as hh
 
-    global BATCH
-    BATCH = args.batch
+    batch = args.batch
 
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    stream = torch.cuda.current_stream()
-    ctx = hh.Context(local, stream=stream.cuda_stream)
+    sampler = ClockSampler(local).__enter__()  # start nvidia-smi before any timing
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
+    ctx = hh.Context(local, stream=st.cuda_stream)
     plans = [hh.Plan.helmholtz(ctx, 2, N, o, k) for o, k in COMBOS]
-    f_host = sources(BATCH, index=1 + rank)
+    f_host = sources(batch, index=1 + rank)
     f = torch.from_numpy(f_host).cuda()
     u = torch.empty_like(f)
     torch.cuda.synchronize()
@@ -210,36 +211,53 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    def step(s):
-        plans[s % len(plans)].solve_source(f, u, BATCH)
-
     for s in range(args.warmup):
-        step(s)
+        plans[s % len(plans)].solve_source(f, u, batch)
     ctx.synchronize()
-    ctx.stage_times()  # discard
-    ctx.set_stage_timing(True)
-    barrier()
+
+    # one CUDA graph per (order, k): a step is a single graph launch, so host-side stalls cannot
+    # open gaps inside the timed region
+    graphs = []
     l0 = ctx.launches
+    for p in plans:
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=st):
+            p.solve_source(f, u, batch)
+        graphs.append(g)
+    kernels_per_step = (ctx.launches - l0) // len(plans)
+    for g in graphs:
+        g.replay()
+    t_wait = time.time()
+    while not sampler.rows and time.time() - t_wait < 10:
+        time.sleep(0.05)
+    sampler.rows.clear()
+    barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        e0.record(stream)
-        for s in range(args.steps):
-            step(s)
-        e1.record(stream)
-        barrier()
-    launches = ctx.launches - l0
-    ctx.set_stage_timing(False)
-    stage_ms, timed = ctx.stage_times()
-    ctx.synchronize()
+    e0.record(st)
+    for s in range(args.steps):
+        graphs[s % len(graphs)].replay()
+    e1.record(st)
+    barrier()
+    sampler.__exit__()
+    clk = sampler
+    launches = kernels_per_step * args.steps
     ms = e0.elapsed_time(e1)
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
-    value = world * BATCH * args.steps / (ms_max / 1000.0)
+    value = world * batch * args.steps / (ms_max / 1000.0)
+
+    # per-kernel device time: a second pass with CUDA events around each stage on the same stream
+    ctx.stage_times()
+    ctx.set_stage_timing(True)
+    for s in range(args.steps):
+        plans[s % len(plans)].solve_source(f, u, batch)
+    ctx.set_stage_timing(False)
+    stage_ms, timed = ctx.stage_times()
 
     # roofline of the dominant kernel (stage with the largest device time)
-    pts = N * N * BATCH
+    pts = N * N * batch
     stage_names = ["dst_forward(k_dst1)", "line_solve(k_line_solve)", "dst_inverse(k_dst1)"]
     dom = int(np.argmax(stage_ms))
     per_launch_ms = stage_ms[dom] / max(1, timed)
@@ -253,23 +271,23 @@ def main():
         pass
 
     # end to end through the public host API (pinned host buffers, copies inside the region)
-    io_bytes = BATCH * N * N * 16
+    io_bytes = batch * N * N * 16
     e2e_steps, e2e_value = 0, None
     if not args.no_e2e:
         pin_in = torch.from_numpy(f_host).pin_memory()
         pin_out = torch.empty_like(pin_in).pin_memory()
         e2e_steps = max(2, min(args.steps, 6))
-        hh.check(hh.lib().hh_solve_source_host(plans[0].h, pin_in.data_ptr(), pin_out.data_ptr(), BATCH), "e2e")
+        hh.check(hh.lib().hh_solve_source_host(plans[0].h, pin_in.data_ptr(), pin_out.data_ptr(), batch), "e2e")
         barrier()
         t0 = time.perf_counter()
         for s in range(e2e_steps):
             p = plans[s % len(plans)]
-            hh.check(hh.lib().hh_solve_source_host(p.h, pin_in.data_ptr(), pin_out.data_ptr(), BATCH), "e2e")
+            hh.check(hh.lib().hh_solve_source_host(p.h, pin_in.data_ptr(), pin_out.data_ptr(), batch), "e2e")
         barrier()
         e2e_s = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
         if world > 1:
             dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
-        e2e_value = world * BATCH * e2e_steps / float(e2e_s.item())
+        e2e_value = world * batch * e2e_steps / float(e2e_s.item())
 
     if rank == 0:
         line = {
@@ -277,7 +295,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded sine modes + CN(0,1e-3) noise)",
-            "config": {"workload": WORKLOAD, "n": N, "batch_per_gpu": BATCH, "orders": [4, 6],
+            "config": {"workload": WORKLOAD, "n": N, "batch_per_gpu": batch, "orders": [4, 6],
                        "k": [10, 50, 200], "form": "plain FP64", "rhs_assembly": "fused",
                        "l2": "inputs 1.07 GB per step > 126 MB L2 (no flush needed)",
                        "parallelism": f"replicas x{world}"},
@@ -289,6 +307,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": io_bytes,
                     "d2h_bytes_per_step": io_bytes, "steps": e2e_steps},
             "gpu_launches": launches,
+            "timing": "CUDA events on the launch stream around CUDA-graph replays (one graph per (order, k))",
             "clocks": clk.summary(),
         }
         if world == 1 and not args.no_cpu_baseline:

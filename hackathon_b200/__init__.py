@@ -100,13 +100,17 @@ class Context:
     """One device + one CUDA stream (include/hh.h hh_ctx)."""
 
     def __init__(self, device: int = 0, stream: int | None = None):
+        import weakref
         p = _vp()
         check(lib().hh_ctx_create(device, stream, C.byref(p)), "hh_ctx_create")
         self.h = p
         self.device = device
+        self.plans = weakref.WeakSet()
 
     def close(self):
         if self.h:
+            for plan in list(self.plans):  # the C context releases them with itself
+                plan.h = None
             lib().hh_ctx_destroy(self.h)
             self.h = None
 
@@ -158,6 +162,7 @@ class Plan:
     def __init__(self, ctx: Context, handle, dim: int, shape: tuple):
         self.ctx, self.h, self.dim, self.shape = ctx, handle, dim, shape
         self.field = int(lib().hh_plan_field_size(handle))
+        ctx.plans.add(self)
 
     @classmethod
     def from_coefficients_2d(cls, ctx: Context, nx: int, ny: int, coef: dict):
@@ -185,9 +190,9 @@ class Plan:
         return cls(ctx, p, 3, (n, n, n))
 
     def close(self):
-        if self.h:
+        if self.h and self.ctx.h:
             lib().hh_plan_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:

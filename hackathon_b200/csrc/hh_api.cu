@@ -10,6 +10,7 @@
 
 #include <math.h>
 #include <stdarg.h>
+#include <stdlib.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -53,6 +54,7 @@ static int upload(Ctx *c, void *dst, const void *src, size_t bytes) {
 using namespace hh;
 
 static void drain_events(Ctx &c);
+static int stage_mark(Ctx &c, int k);
 
 // ------------------------------------------------------------------ library ------
 extern "C" const char *hh_last_error(void) { return g_err.c_str(); }
@@ -86,11 +88,20 @@ extern "C" int hh_ctx_create(int device, void *stream, hh_ctx **out) {
     return HH_OK;
 }
 
+static void plan_free(hh_plan *pl);
+
 extern "C" int hh_ctx_destroy(hh_ctx *x) {
     if (!x) return HH_OK;
     cudaSetDevice(x->c.device);
     cudaStreamSynchronize(x->c.stream);
     drain_events(x->c);
+    // plans still alive belong to this context: release them with it
+    for (Plan *p : x->c.plans) {
+        hh_plan *pl = reinterpret_cast<hh_plan *>(p); // Plan is the first member of hh_plan
+        plan_free(pl);
+        delete pl;
+    }
+    x->c.plans.clear();
     for (auto &kv : x->c.tw) cudaFree(kv.second);
     for (auto &kv : x->c.sn) cudaFree(kv.second);
     for (auto &kv : x->c.dense) cudaFree(kv.second);
@@ -124,6 +135,7 @@ extern "C" int hh_ctx_synchronize(hh_ctx *x) {
 extern "C" long long hh_ctx_launch_count(const hh_ctx *x) { return x ? x->c.launches : 0; }
 
 static void drain_events(Ctx &c) {
+    if (!c.ev_pending.empty()) cudaEventSynchronize(c.ev_pending.back()); // all recorded events complete
     for (size_t g = 0; g + 4 <= c.ev_pending.size(); g += 4) {
         float t;
         for (int s = 0; s < 3; s++) {
@@ -226,18 +238,27 @@ extern "C" int hh_dst2_planes(hh_ctx *x, int nx, int ny, long nplanes, const dou
 // -------------------------------------------------------------------- plans ------
 static int plan_alloc(hh_plan *pl) {
     Plan &p = pl->p;
-    HH_CUDA(cudaMalloc(&p.Lf, sizeof(double2) * (size_t)p.lines * p.rows));
-    HH_CUDA(cudaMalloc(&p.Ui, sizeof(double2) * (size_t)p.lines * p.rows));
-    HH_CUDA(cudaMalloc(&p.rowc, sizeof(double2) * 4 * (size_t)p.rows));
+    p.ctx->plans.push_back(&p);
+    HH_CUDA(cudaMalloc(&p.Pv, sizeof(double2) * (size_t)segment_count(p.rows) * p.lines));
+    p.prow = padded_rows(p.rows);
+    HH_CUDA(cudaMalloc(&p.rowc, sizeof(double2) * 4 * (size_t)p.prow));
+    HH_CUDA(cudaMalloc(&p.subt, sizeof(double2) * 4 * (size_t)p.prow));
+    HH_CUDA(cudaMalloc(&p.diagt, sizeof(double2) * 4 * (size_t)p.prow));
     HH_CUDA(cudaMalloc(&p.mu, sizeof(double) * 3 * (size_t)p.lines));
     return HH_OK;
 }
 
 static void plan_free(hh_plan *pl) {
     Plan &p = pl->p;
-    cudaFree(p.Lf);
-    cudaFree(p.Ui);
+    if (p.ctx) {
+        auto &v = p.ctx->plans;
+        for (size_t i = 0; i < v.size(); i++)
+            if (v[i] == &p) { v.erase(v.begin() + (long)i); break; }
+    }
+    cudaFree(p.Pv);
     cudaFree(p.rowc);
+    cudaFree(p.subt);
+    cudaFree(p.diagt);
     cudaFree(p.mu);
     cudaFree(p.pade_l);
     cudaFree(p.pade_u);
@@ -250,7 +271,7 @@ static void plan_free(hh_plan *pl) {
 // U_r = 10 - L_r; the device keeps L_r (L_0 = 0) and 1/U_r.
 static int plan_pade(hh_plan *pl) {
     Plan &p = pl->p;
-    std::vector<double> L(p.rows), Ui(p.rows);
+    std::vector<double> L(p.prow, 0.0), Ui(p.prow, 0.0); // zero past the line (neutral rows)
     double U = 10.0;
     L[0] = 0.0;
     Ui[0] = 1.0 / U;
@@ -259,10 +280,10 @@ static int plan_pade(hh_plan *pl) {
         U = 10.0 - L[r];
         Ui[r] = 1.0 / U;
     }
-    HH_CUDA(cudaMalloc(&p.pade_l, sizeof(double) * (size_t)p.rows));
-    HH_CUDA(cudaMalloc(&p.pade_u, sizeof(double) * (size_t)p.rows));
-    HH_CUDA(cudaMemcpy(p.pade_l, L.data(), sizeof(double) * (size_t)p.rows, cudaMemcpyHostToDevice));
-    HH_CUDA(cudaMemcpy(p.pade_u, Ui.data(), sizeof(double) * (size_t)p.rows, cudaMemcpyHostToDevice));
+    HH_CUDA(cudaMalloc(&p.pade_l, sizeof(double) * (size_t)p.prow));
+    HH_CUDA(cudaMalloc(&p.pade_u, sizeof(double) * (size_t)p.prow));
+    HH_CUDA(cudaMemcpy(p.pade_l, L.data(), sizeof(double) * (size_t)p.prow, cudaMemcpyHostToDevice));
+    HH_CUDA(cudaMemcpy(p.pade_u, Ui.data(), sizeof(double) * (size_t)p.prow, cudaMemcpyHostToDevice));
     return HH_OK;
 }
 
@@ -271,18 +292,31 @@ static int plan_factor(hh_plan *pl, const std::vector<double2> &sub, const std::
                        const std::vector<double2> &sup, const std::vector<double> &mu) {
     Plan &p = pl->p;
     Ctx  *c = p.ctx;
-    double2 *dsub = nullptr, *ddia = nullptr;
-    const size_t tb = sizeof(double2) * 4 * (size_t)p.rows;
-    HH_CUDA(cudaMalloc(&dsub, tb));
-    HH_CUDA(cudaMalloc(&ddia, tb));
-    int rc = upload(c, dsub, sub.data(), tb);
-    if (rc == HH_OK) rc = upload(c, ddia, dia.data(), tb);
-    if (rc == HH_OK) rc = upload(c, p.rowc, sup.data(), tb);
+    // constant-coefficient lines (constant k): every row of the three tables equals row 0
+    auto constant = [&](const std::vector<double2> &t) {
+        for (int k = 0; k < 4; k++)
+            for (int r = 1; r < p.rows; r++) {
+                const double2 a0 = t[(size_t)k * p.rows], ar = t[(size_t)k * p.rows + r];
+                if (a0.x != ar.x || a0.y != ar.y) return false;
+            }
+        return true;
+    };
+    p.const_rows = constant(sub) && constant(dia) && constant(sup);
+    // tables are [4][prow], zero past the last row (neutral rows in the solve)
+    auto padded = [&](const std::vector<double2> &t) {
+        std::vector<double2> o(4 * (size_t)p.prow, make_double2(0.0, 0.0));
+        for (int k = 0; k < 4; k++)
+            for (int r = 0; r < p.rows; r++) o[(size_t)k * p.prow + r] = t[(size_t)k * p.rows + r];
+        return o;
+    };
+    const std::vector<double2> psub = padded(sub), pdia = padded(dia), psup = padded(sup);
+    const size_t tb = sizeof(double2) * 4 * (size_t)p.prow;
+    int rc = upload(c, p.subt, psub.data(), tb);
+    if (rc == HH_OK) rc = upload(c, p.diagt, pdia.data(), tb);
+    if (rc == HH_OK) rc = upload(c, p.rowc, psup.data(), tb);
     if (rc == HH_OK) rc = upload(c, p.mu, mu.data(), sizeof(double) * 3 * (size_t)p.lines);
-    if (rc == HH_OK) rc = launch_factor(&p, dsub, ddia, p.rowc);
+    if (rc == HH_OK) rc = launch_factor(&p, p.subt, p.diagt, p.rowc);
     cudaError_t e = cudaStreamSynchronize(c->stream);
-    cudaFree(dsub);
-    cudaFree(ddia);
     if (rc != HH_OK) return rc;
     if (e != cudaSuccess) return cuda_fail(e, "factorisation", __FILE__, __LINE__);
     return HH_OK;

@@ -224,13 +224,17 @@ __device__ __forceinline__ double2 slot_scan_inclusive(double2 x, int t, int slo
 }
 
 // ------------------------------------------------------------------- kernel -------
-// STRIDED = false: line s of the CTA is row (blockIdx.x*S + s), contiguous, at in + row*in_ld.
-// STRIDED = true : line s is column (blockIdx.x*S + s) of plane blockIdx.y; element j at
-//                  in + plane*plane_stride + col + j*in_ld (same addressing for out).
-template <int M, bool STRIDED>
+// Line s of the CTA is line (blockIdx.x*S + s) of plane blockIdx.y.  Its element j lives at
+//   IN_STRIDED = false:  in + plane*in_plane + line*in_ld + j        (contiguous rows)
+//   IN_STRIDED = true :  in + plane*in_plane + line + j*in_ld        (columns; S neighbouring
+//                        lines are loaded together, S*16 contiguous bytes per j)
+// and likewise for the output with OUT_STRIDED / out_ld / out_plane.  Rows in + columns out
+// writes the transform transposed (each output line contiguous in the other direction).
+template <int M, bool IN_STRIDED, bool OUT_STRIDED>
 __global__ void __launch_bounds__(DstGeom<M>::NT)
     k_dst1(const double2 *__restrict__ in, double2 *__restrict__ out, long nlines, long in_ld, long out_ld,
-           long plane_stride, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
+           long in_plane, long out_plane, const double2 *__restrict__ tw, const double *__restrict__ sn,
+           int *err) {
     using G = DstGeom<M>;
     constexpr int T = G::T, R = G::R, S = G::S, N = M - 1;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -242,16 +246,16 @@ __global__ void __launch_bounds__(DstGeom<M>::NT)
 
     const long line = (long)blockIdx.x * S + slot;
     const bool live = line < nlines;
-    const long pbase = STRIDED ? (long)blockIdx.y * plane_stride : 0;
+    const long ibase = (long)blockIdx.y * in_plane, obase = (long)blockIdx.y * out_plane;
 
     // ---- stage the line into shared memory (unpadded, x_j at buf[j-1])
-    if constexpr (!STRIDED) {
+    if constexpr (!IN_STRIDED) {
         if (threadIdx.x < S) mbar_init(&bars[threadIdx.x], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         __syncthreads();
         if (t == 0 && live) {
             mbar_expect_tx(&bars[slot], N * 16);
-            tma_bulk_load(buf, in + line * in_ld, N * 16, &bars[slot]);
+            tma_bulk_load(buf, in + ibase + line * in_ld, N * 16, &bars[slot]);
         }
         if (live) {
             // A copy that never lands is reported through `err`; the slot keeps going so that
@@ -266,7 +270,7 @@ __global__ void __launch_bounds__(DstGeom<M>::NT)
         for (int idx = threadIdx.x; idx < S * N; idx += G::NT) {
             const int c = idx % S, j = idx / S;
             double2  *b2 = reinterpret_cast<double2 *>(smem + G::HDR + c * G::SLOT_BYTES);
-            b2[j] = (col0 + c < nlines) ? in[pbase + col0 + c + (long)j * in_ld] : make_double2(0.0, 0.0);
+            b2[j] = (col0 + c < nlines) ? in[ibase + col0 + c + (long)j * in_ld] : make_double2(0.0, 0.0);
         }
         __syncthreads();
     }
@@ -327,10 +331,10 @@ __global__ void __launch_bounds__(DstGeom<M>::NT)
     }
 
     // ---- write back
-    if constexpr (!STRIDED) {
+    if constexpr (!OUT_STRIDED) {
         slot_sync<T>(slot);
         if (live) {
-            double2 *dst = out + line * out_ld;
+            double2 *dst = out + obase + line * out_ld;
 #pragma unroll
             for (int u = 0; u < R; u++) {
                 const int i = t + T * u;
@@ -343,7 +347,7 @@ __global__ void __launch_bounds__(DstGeom<M>::NT)
         for (int idx = threadIdx.x; idx < S * N; idx += G::NT) {
             const int c = idx % S, j = idx / S;
             const double2 *b2 = reinterpret_cast<const double2 *>(smem + G::HDR + c * G::SLOT_BYTES);
-            if (col0 + c < nlines) out[pbase + col0 + c + (long)j * out_ld] = b2[pad_idx(j)];
+            if (col0 + c < nlines) out[obase + col0 + c + (long)j * out_ld] = b2[pad_idx(j)];
         }
     }
 }
@@ -434,65 +438,75 @@ int dense_for(Ctx *c, int n, const double **mat) {
 }
 
 // -------------------------------------------------------------------- launch ------
-template <int M, bool STRIDED>
-static int launch_fft(Ctx *c, const double2 *in, double2 *out, long nlines, long planes, long in_ld, long out_ld,
-                      long plane_stride) {
+struct DstArgs {
+    const double2 *in;
+    double2       *out;
+    long           nlines, planes, in_ld, out_ld, in_plane, out_plane;
+};
+
+template <int M, bool IS, bool OS> static int launch_fft(Ctx *c, const DstArgs &a) {
     using G = DstGeom<M>;
     const double2 *tw;
     const double  *sn;
     HH_TRY(tables_for(c, M, &tw, &sn));
-    HH_CUDA(cudaFuncSetAttribute(k_dst1<M, STRIDED>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
-    dim3 grid((unsigned)((nlines + G::S - 1) / G::S), (unsigned)planes);
-    k_dst1<M, STRIDED><<<grid, G::NT, G::SMEM, c->stream>>>(in, out, nlines, in_ld, out_ld, plane_stride, tw, sn,
-                                                             c->err_word);
+    HH_CUDA(cudaFuncSetAttribute(k_dst1<M, IS, OS>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
+    dim3 grid((unsigned)((a.nlines + G::S - 1) / G::S), (unsigned)a.planes);
+    k_dst1<M, IS, OS><<<grid, G::NT, G::SMEM, c->stream>>>(a.in, a.out, a.nlines, a.in_ld, a.out_ld, a.in_plane,
+                                                            a.out_plane, tw, sn, c->err_word);
     HH_CUDA(cudaGetLastError());
     c->launches++;
     return HH_OK;
 }
 
-template <bool STRIDED>
-static int launch_dispatch(Ctx *c, int n, const double2 *in, double2 *out, long nlines, long planes, long in_ld,
-                           long out_ld, long plane_stride) {
+template <bool IS, bool OS> static int launch_dispatch(Ctx *c, int n, const DstArgs &a) {
     if (n < 1) { set_error("DST length must be >= 1 (got %d)", n); return HH_ERR_INVALID; }
-    if (!STRIDED && ((((uintptr_t)in) & 15) || (((uintptr_t)out) & 15))) {
+    if (a.nlines <= 0 || a.planes <= 0) return HH_OK;
+    if (a.planes > 65535) { set_error("DST: too many planes (%ld)", a.planes); return HH_ERR_INVALID; }
+    if (!IS && (((uintptr_t)a.in) & 15)) {
         set_error("DST rows must be 16-byte aligned");
         return HH_ERR_INVALID;
     }
     switch (n + 1) {
-    case 64: return launch_fft<64, STRIDED>(c, in, out, nlines, planes, in_ld, out_ld, plane_stride);
-    case 128: return launch_fft<128, STRIDED>(c, in, out, nlines, planes, in_ld, out_ld, plane_stride);
-    case 256: return launch_fft<256, STRIDED>(c, in, out, nlines, planes, in_ld, out_ld, plane_stride);
-    case 512: return launch_fft<512, STRIDED>(c, in, out, nlines, planes, in_ld, out_ld, plane_stride);
-    case 1024: return launch_fft<1024, STRIDED>(c, in, out, nlines, planes, in_ld, out_ld, plane_stride);
-    case 2048: return launch_fft<2048, STRIDED>(c, in, out, nlines, planes, in_ld, out_ld, plane_stride);
-    case 4096: return launch_fft<4096, STRIDED>(c, in, out, nlines, planes, in_ld, out_ld, plane_stride);
-    case 8192: return launch_fft<8192, STRIDED>(c, in, out, nlines, planes, in_ld, out_ld, plane_stride);
+    case 64: return launch_fft<64, IS, OS>(c, a);
+    case 128: return launch_fft<128, IS, OS>(c, a);
+    case 256: return launch_fft<256, IS, OS>(c, a);
+    case 512: return launch_fft<512, IS, OS>(c, a);
+    case 1024: return launch_fft<1024, IS, OS>(c, a);
+    case 2048: return launch_fft<2048, IS, OS>(c, a);
+    case 4096: return launch_fft<4096, IS, OS>(c, a);
+    case 8192: return launch_fft<8192, IS, OS>(c, a);
     default: break;
     }
     if (n > 4096) {
         set_error("DST length %d: n+1 must be a power of two (64..8192) or n <= 4096", n);
         return HH_ERR_UNSUPPORTED;
     }
+    if (IS != OS) {
+        set_error("DST length %d: transposing modes need n+1 a power of two", n);
+        return HH_ERR_UNSUPPORTED;
+    }
     const double *mat;
     HH_TRY(dense_for(c, n, &mat));
     const size_t shm = sizeof(double2) * (size_t)n;
-    if (shm > 48 * 1024) HH_CUDA(cudaFuncSetAttribute(k_dst1_dense<STRIDED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-    dim3 grid((unsigned)nlines, (unsigned)planes);
-    k_dst1_dense<STRIDED><<<grid, kDenseThreads, shm, c->stream>>>(in, out, n, nlines, in_ld, out_ld, plane_stride, mat);
+    if (shm > 48 * 1024)
+        HH_CUDA(cudaFuncSetAttribute(k_dst1_dense<IS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    dim3 grid((unsigned)a.nlines, (unsigned)a.planes);
+    k_dst1_dense<IS><<<grid, kDenseThreads, shm, c->stream>>>(a.in, a.out, n, a.nlines, a.in_ld, a.out_ld,
+                                                              a.in_plane, mat);
     HH_CUDA(cudaGetLastError());
     c->launches++;
     return HH_OK;
 }
 
 int launch_dst_rows(Ctx *c, int n, long rows, const double2 *in, long in_ld, double2 *out, long out_ld) {
-    if (rows <= 0) return HH_OK;
-    return launch_dispatch<false>(c, n, in, out, rows, 1, in_ld, out_ld, 0);
+    DstArgs a{in, out, rows, 1, in_ld, out_ld, 0, 0};
+    return launch_dispatch<false, false>(c, n, a);
 }
 
 int launch_dst_cols(Ctx *c, int n, long ncols, long planes, const double2 *in, long ld, long plane_stride,
                     double2 *out) {
-    if (ncols <= 0 || planes <= 0) return HH_OK;
-    return launch_dispatch<true>(c, n, in, out, ncols, planes, ld, ld, plane_stride);
+    DstArgs a{in, out, ncols, planes, ld, ld, plane_stride, plane_stride};
+    return launch_dispatch<true, true>(c, n, a);
 }
 
 } // namespace hh

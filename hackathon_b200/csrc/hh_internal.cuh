@@ -92,15 +92,16 @@ struct Plan {
     // line-solve geometry: `lines` independent lines of `rows` points; element (row r, line q)
     // at offset r*row_stride + q inside one right-hand side.
     int    lines = 0, rows = 0;
+    int    prow = 0;                // rows of the (zero-padded) per-row tables
     long   row_stride = 0;
     long   field = 0;               // complex elements per right-hand side
-    // factors in [row][line] layout (line fastest): Lf = sub-diagonal multiplier, Ui = 1/pivot
-    double2 *Lf = nullptr, *Ui = nullptr;
-    // super-diagonal Up(row, line) = sum_t rowc[t][row] * mu[t][line] + rowc[3][row]
+    // reciprocal Thomas pivot of the row before each 16-row segment, [segment][line]
+    double2 *Pv = nullptr;
+    bool     const_rows = false; // stencil row tables constant along the line
+    double2 *subt = nullptr, *diagt = nullptr; // sub/diagonal row tables (4 * rows each)
+    // super-diagonal(row, line) = rowc[0][row] mu[0][line] + rowc[1][row] mu[1][line] + rowc[2][row] mu[2][line] + rowc[3][row]
     double2 *rowc = nullptr;        // 4 * rows complex
     double  *mu = nullptr;          // 3 * lines real
-    double2 *scratch = nullptr;     // one field per batch slot (transformed data)
-    int      scratch_batch = 0;
     // fused source operator (homogeneous Dirichlet, constant k): 0 = off
     int      src_order = 0;
     double  *pade_l = nullptr, *pade_u = nullptr; // [1 10 1] factors along the line (rows each)
@@ -114,5 +115,8 @@ int launch_dst_cols(Ctx *c, int n, long ncols, long planes, const double2 *in, l
 int launch_factor(Plan *p, const double2 *subt, const double2 *diagt, const double2 *supt);
 int launch_line_solve(Plan *p, const double2 *in, double2 *out, int batch, int src_order);
 int read_device_error(Ctx *c, int *val);
+int segment_count(int rows);
+int padded_rows(int rows);
+
 
 } // namespace hh

@@ -22,24 +22,33 @@
 // recurrence  L_0 = 0, P_0 = diag_0,  L_r = sub_r / P_{r-1},  P_r = diag_r - L_r super_{r-1};
 // the device keeps L_r and 1/P_r in [row][line] layout.
 //
-// Solve (per right-hand side): each thread owns a segment of MSEG consecutive rows of one line
-// in registers.  Forward substitution y_r = f_r - L_r y_{r-1} and back substitution
-// x_r = y_r/P_r - (super_r/P_r) x_{r+1} are first-order linear recurrences; each segment
-// applies its rows as an affine map of the value entering it, the maps are composed across the
-// segments of a line by a Kogge-Stone scan in shared memory, and every segment then re-runs its
-// rows from the exact entering value.  All values stay on chip: one HBM read and one HBM write
-// per point.
+// Solve: each thread owns a segment of kSeg = 8 consecutive rows of one line.  Only the
+// reciprocal pivot entering each segment is stored by the set-up; the thread re-runs the
+// factor recurrence for its own rows into registers (the same arithmetic, so the factors are
+// those of the sequential factorisation) and keeps them for every right-hand side of its
+// chunk.  Forward substitution y_r = f_r - L_r y_{r-1} and back substitution
+// x_r = (y_r - super_r x_{r+1}) / P_r are first-order linear recurrences: each segment applies
+// its rows as an affine map y_out = A y_in + B of the value entering it.  A (product of the
+// segment's multipliers) depends on the factors only; B comes from a local sweep.  The maps of
+// a line are composed across its segments by a warp-shuffle scan plus one cross-warp level in
+// shared memory, and every segment then re-runs its rows from the exact entering value.  The
+// next right-hand side is prefetched into shared memory with cp.async while the current one
+// is solved.  One HBM read and one HBM write per point; no per-point factor traffic.
 //
 // Fused right-hand-side operator (plans for the constant-k, homogeneous-Dirichlet class).  The
 // compact RHS of 2D_Program/main_functions/rhs.c:4-97 and 3D_Program/main_functions/rhs.c:13-166
 // is a polynomial in the 1D second-difference and Pade operators of each direction.  In the
 // DST basis of the transformed direction(s) those operators are diagonal (second difference ->
 // lambda - 2, Pade [1 10 1] -> 10 + lambda), so after the forward DST the RHS of line q is
-//     F = h^2 [ alpha g + beta D2 g + gamma (omega/12 + D2 omega/360) ],  omega = T^-1 (12 D2 g)
+//     order 6:  F = h^2 [ alpha g + beta D2 g + omega/12 + D2 omega/360 ],  omega = T^-1 (12 D2 g)
 // where g is the transformed source along the line, D2 the second difference along the line
-// (zero boundary values), T = tridiag(1, 10, 1) the Pade matrix of the line direction, and
-// alpha, beta, gamma depend on the order and on the line's eigenvalues.  It is applied in
-// registers before the Helmholtz solve, so the RHS assembly costs no extra HBM traffic.
+// (zero boundary values), T = tridiag(1, 10, 1) = D2 + 12 I the Pade matrix of the line
+// direction, and alpha, beta depend on k and on the line's eigenvalues.  Because T = D2 + 12 I,
+// omega = 12 g - 144 T^-1 g and D2 omega = 12 D2 g - 144 g + 1728 T^-1 g, so
+//     order 6:  F = h^2 [ (alpha + 0.6) g + (beta + 1/30) D2 g - 7.2 T^-1 g ]
+//     order 4:  F = h^2 [ alpha g + D2 g / 12 ],    order 2:  F = h^2 g
+// It is applied in registers before the Helmholtz solve, so the RHS assembly costs no extra
+// HBM traffic.
 #include "hh_internal.cuh"
 
 namespace hh {
@@ -57,302 +66,423 @@ __device__ __forceinline__ double2 shifted(const double2 *__restrict__ tab, int 
 }
 
 // ----------------------------------------------------------------- factors --------
-__global__ void k_factor(int lines, int rows, const double *__restrict__ mu, const double2 *__restrict__ subt,
-                         const double2 *__restrict__ diagt, const double2 *__restrict__ supt,
-                         double2 *__restrict__ Lf, double2 *__restrict__ Ui) {
+constexpr int kSeg = 8;          // rows per thread in the solve
+constexpr int kLineThreads = 512;
+constexpr int kWarps = kLineThreads / 32;
+constexpr int kMinSegments = 16; // at most 32 lines per CTA
+
+// One step of the factor recurrence, shared by the set-up and the solve so both produce the
+// same values: L = sub / P_prev (as sub * (1/P_prev)), P = diag - L super_prev, returns 1/P.
+__device__ __forceinline__ double2 factor_step(double2 sub, double2 dia, double2 sup_prev, double2 ui_prev,
+                                               double2 &L) {
+    L = make_double2(fma(sub.x, ui_prev.x, -(sub.y * ui_prev.y)), fma(sub.x, ui_prev.y, sub.y * ui_prev.x));
+    const double2 P = make_double2(dia.x - fma(L.x, sup_prev.x, -(L.y * sup_prev.y)),
+                                   dia.y - fma(L.x, sup_prev.y, L.y * sup_prev.x));
+    const double  d = 1.0 / fma(P.x, P.x, P.y * P.y);
+    return make_double2(P.x * d, -P.y * d);
+}
+__device__ __forceinline__ double2 first_pivot(double2 dia) {
+    const double d = 1.0 / fma(dia.x, dia.x, dia.y * dia.y);
+    return make_double2(dia.x * d, -dia.y * d);
+}
+
+// One thread per line: runs the Thomas recurrence over the whole line (the reference's LU(),
+// 2D LU.c:25-40 / 3D LU.c:51-72) and keeps 1/P of the row before each kSeg-row segment.
+__global__ void k_factor(int lines, int rows, int prow, const double *__restrict__ mu,
+                         const double2 *__restrict__ subt, const double2 *__restrict__ diagt,
+                         const double2 *__restrict__ supt, double2 *__restrict__ Pv) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= lines) return;
     const double m0 = mu[q], m1 = mu[lines + q], m2 = mu[2 * lines + q];
-    double2 piv = shifted(diagt, rows, 0, m0, m1, m2);
-    double2 up_prev = shifted(supt, rows, 0, m0, m1, m2);
-    Lf[q] = make_double2(0.0, 0.0);
-    Ui[q] = crcp(piv);
+    double2 ui = first_pivot(shifted(diagt, prow, 0, m0, m1, m2));
+    double2 up_prev = shifted(supt, prow, 0, m0, m1, m2);
+    Pv[q] = make_double2(0.0, 0.0);
     for (int r = 1; r < rows; r++) {
-        const double2 sub = shifted(subt, rows, r, m0, m1, m2);
-        const double2 dia = shifted(diagt, rows, r, m0, m1, m2);
-        const double2 L = cdiv(sub, piv);
-        piv = cfms(dia, L, up_prev);
-        const long o = (long)r * lines + q;
-        Lf[o] = L;
-        Ui[o] = crcp(piv);
-        up_prev = shifted(supt, rows, r, m0, m1, m2);
+        if (r % kSeg == 0) Pv[(long)(r / kSeg) * lines + q] = ui;
+        double2 L;
+        ui = factor_step(shifted(subt, prow, r, m0, m1, m2), shifted(diagt, prow, r, m0, m1, m2), up_prev, ui, L);
+        up_prev = shifted(supt, prow, r, m0, m1, m2);
     }
 }
 
 int launch_factor(Plan *p, const double2 *subt, const double2 *diagt, const double2 *supt) {
     const int nt = 128;
-    k_factor<<<(p->lines + nt - 1) / nt, nt, 0, p->ctx->stream>>>(p->lines, p->rows, p->mu, subt, diagt, supt, p->Lf,
-                                                                   p->Ui);
+    k_factor<<<(p->lines + nt - 1) / nt, nt, 0, p->ctx->stream>>>(p->lines, p->rows, p->prow, p->mu, subt, diagt,
+                                                                   supt, p->Pv);
     HH_CUDA(cudaGetLastError());
     p->ctx->launches++;
     return HH_OK;
 }
 
 // ------------------------------------------------------------------- solve --------
-constexpr int kSolveThreads = 512;
+// Thread (c, s): line c of the CTA (fastest), segment s.  A warp holds all CW lines and
+// SPW = 32/CW consecutive segments of each, so a line's segments are spread over the warps.
+struct Lane {
+    int c, s, sl, w, lane, CW, SPW;
+};
 
-// Inclusive scan of affine maps (A, B) over the P segments of each of the CW lines of the CTA.
-// Thread (c, s) sits at tid = c + CW*s.  FORWARD combines left-to-right, otherwise right-to-left.
-// Returns the value entering this thread's segment (B of the neighbour's inclusive prefix).
-template <bool FORWARD>
-__device__ __forceinline__ double2 segment_scan(double2 A, double2 B, int c, int s, int CW, int P, double2 *sA,
-                                                double2 *sB) {
-    const int pos = FORWARD ? s : (P - 1 - s);
-    const int me = c + CW * pos;
-    sA[me] = A;
-    sB[me] = B;
-    __syncthreads();
-    for (int d = 1; d < P; d <<= 1) {
-        double2 Al = make_double2(0.0, 0.0), Bl = make_double2(0.0, 0.0);
-        const bool has = pos >= d;
-        if (has) {
-            Al = sA[me - CW * d];
-            Bl = sB[me - CW * d];
-        }
-        __syncthreads();
-        if (has) {
-            B = cfma(B, A, Bl); // apply the earlier map first: y = A (Al y0 + Bl) + B
+__device__ __forceinline__ double2 shfl_up2(double2 v, int off) {
+    return make_double2(__shfl_up_sync(0xffffffffu, v.x, off), __shfl_up_sync(0xffffffffu, v.y, off));
+}
+__device__ __forceinline__ double2 shfl_down2(double2 v, int off) {
+    return make_double2(__shfl_down_sync(0xffffffffu, v.x, off), __shfl_down_sync(0xffffffffu, v.y, off));
+}
+
+struct ScanSmem {
+    double2 A[2][kWarps][32], B[2][kWarps][32]; // cross-warp totals / neighbour values (double buffered)
+};
+
+// Value entering segment s for the left-to-right composition of maps (A, B): y = A y_in + B.
+__device__ __forceinline__ double2 scan_forward(double2 A, double2 B, const Lane &L, ScanSmem &sm, int par) {
+    for (int off = L.CW; off < 32; off <<= 1) {
+        const double2 Al = shfl_up2(A, off), Bl = shfl_up2(B, off);
+        if (L.lane >= off) {
+            B = cfma(B, A, Bl);
             A = cmul(A, Al);
-            sA[me] = A;
-            sB[me] = B;
         }
-        __syncthreads();
     }
-    const double2 in = (pos > 0) ? sB[me - CW] : make_double2(0.0, 0.0);
-    __syncthreads(); // buffers are reused by the next scan
-    return in;
+    double2 Ae = shfl_up2(A, L.CW), Be = shfl_up2(B, L.CW);
+    if (L.sl == 0) { Ae = make_double2(1.0, 0.0); Be = make_double2(0.0, 0.0); }
+    if (L.sl == L.SPW - 1) { sm.A[par][L.w][L.c] = A; sm.B[par][L.w][L.c] = B; }
+    __syncthreads();
+    double2 E = make_double2(0.0, 0.0);
+    for (int w2 = 0; w2 < L.w; w2++) E = cfma(sm.B[par][w2][L.c], sm.A[par][w2][L.c], E);
+    return cfma(Be, Ae, E);
 }
 
-// Values of the rows just before and just after this thread's segment (zero outside the line).
-template <int SEG>
-__device__ __forceinline__ void segment_neighbours(const double2 (&v)[SEG], int c, int s, int CW, int P,
-                                                   double2 *sA, double2 *sB, double2 &before, double2 &after) {
-    const int me = c + CW * s;
-    sA[me] = v[0];
-    sB[me] = v[SEG - 1];
+// Value entering segment s from the right (maps composed right-to-left).
+__device__ __forceinline__ double2 scan_backward(double2 A, double2 B, const Lane &L, ScanSmem &sm, int par) {
+    for (int off = L.CW; off < 32; off <<= 1) {
+        const double2 Ar = shfl_down2(A, off), Br = shfl_down2(B, off);
+        if (L.lane + off < 32) {
+            B = cfma(B, A, Br);
+            A = cmul(A, Ar);
+        }
+    }
+    double2 Ae = shfl_down2(A, L.CW), Be = shfl_down2(B, L.CW);
+    if (L.sl == L.SPW - 1) { Ae = make_double2(1.0, 0.0); Be = make_double2(0.0, 0.0); }
+    if (L.sl == 0) { sm.A[par][L.w][L.c] = A; sm.B[par][L.w][L.c] = B; }
     __syncthreads();
-    before = (s > 0) ? sB[me - CW] : make_double2(0.0, 0.0);
-    after = (s + 1 < P) ? sA[me + CW] : make_double2(0.0, 0.0);
-    __syncthreads();
+    double2 E = make_double2(0.0, 0.0);
+    for (int w2 = kWarps - 1; w2 > L.w; w2--) E = cfma(sm.B[par][w2][L.c], sm.A[par][w2][L.c], E);
+    return cfma(Be, Ae, E);
 }
+
+// Last value of segment s-1 and first value of segment s+1 (zero outside the line).
+__device__ __forceinline__ void neighbours(double2 lo, double2 hi, const Lane &L, ScanSmem &sm, int par,
+                                           double2 &prev_hi, double2 &next_lo) {
+    prev_hi = shfl_up2(hi, L.CW);
+    next_lo = shfl_down2(lo, L.CW);
+    if (L.sl == L.SPW - 1) sm.B[par][L.w][L.c] = hi;
+    if (L.sl == 0) sm.A[par][L.w][L.c] = lo;
+    __syncthreads();
+    if (L.sl == 0) prev_hi = (L.w > 0) ? sm.B[par][L.w - 1][L.c] : make_double2(0.0, 0.0);
+    if (L.sl == L.SPW - 1) next_lo = (L.w < kWarps - 1) ? sm.A[par][L.w + 1][L.c] : make_double2(0.0, 0.0);
+}
+
+// 16-byte asynchronous global -> shared copy; src_bytes = 0 writes zeros.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 struct SrcParams {
-    int     dim;       // 2 or 3
-    double  h2;        // h^2
-    double2 k2h2_20;   // k^2 h^2 / 20
-    const double *pl;  // Pade [1 10 1] multipliers L_r = 1/U_{r-1} (L_0 = 0), rows
-    const double *pu;  // Pade reciprocal pivots 1/U_r, rows
+    int     dim;      // 2 or 3
+    double  h2;       // h^2
+    double2 k2h2_20;  // k^2 h^2 / 20
+    const double *pl; // Pade [1 10 1] multipliers L_r = 1/U_{r-1} (L_0 = 0); zero past the line
+    const double *pu; // Pade reciprocal pivots 1/U_r; zero past the line
 };
 
 // SRC = 0: the input already is the transformed RHS.  SRC = 2/4/6: the input is the transformed
-// source g and the compact operator of that order is applied first.
-template <int SEG, int SRC>
-__global__ void __launch_bounds__(kSolveThreads)
-    k_line_solve(const double2 *__restrict__ in, double2 *__restrict__ out, int lines, int rows, long row_stride,
-                 long field, int CW, int P, const double2 *__restrict__ Lf, const double2 *__restrict__ Ui,
-                 const double2 *__restrict__ supt, const double *__restrict__ mu, SrcParams sp) {
-    __shared__ double2 sA[kSolveThreads], sB[kSolveThreads];
-    const int tid = threadIdx.x;
-    const int c = tid % CW, s = tid / CW;
-    const int q = blockIdx.x * CW + c;
+// source g and the compact operator of that order is applied first (see the file header).
+// CONST_ROWS: the stencil rows do not vary along the line (constant k).
+// Rows past the end of a line are neutral: zero data, zero reciprocal pivots, zero Pade factors,
+// so the sweeps run without per-row conditions.
+template <int SRC, bool CONST_ROWS>
+__global__ void __launch_bounds__(kLineThreads, 1)
+    k_line_solve(const double2 *__restrict__ in, double2 *__restrict__ out, int lines, int rows, int prow,
+                 long row_stride, long field, int batch, int rb, int CW, const double2 *__restrict__ Pv,
+                 const double2 *__restrict__ subt, const double2 *__restrict__ diagt, const double2 *__restrict__ supt,
+                 const double *__restrict__ mu, SrcParams sp) {
+    __shared__ ScanSmem sm;
+    extern __shared__ double2 pre[]; // [kSeg][kLineThreads] prefetch of the next right-hand side,
+                                     // then (SRC == 6) [kSeg][kLineThreads] Pade scratch
+    double2 *wsm = pre + kSeg * kLineThreads + threadIdx.x;
+    Lane L;
+    L.lane = threadIdx.x & 31;
+    L.w = threadIdx.x >> 5;
+    L.CW = CW;
+    L.SPW = 32 / CW;
+    L.c = threadIdx.x % CW;
+    L.s = threadIdx.x / CW;
+    L.sl = L.lane / CW;
+    const int  q = blockIdx.x * CW + L.c;
     const bool live = q < lines;
-    const int r0 = s * SEG;
-    const long base = (long)blockIdx.y * field;
+    const int  qq = live ? q : 0;
+    const int  r0 = L.s * kSeg;
     const double m0 = live ? mu[q] : 0.0, m1 = live ? mu[lines + q] : 0.0, m2 = live ? mu[2 * lines + q] : 0.0;
+    const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
 
-    double2 v[SEG];
-#pragma unroll
-    for (int u = 0; u < SEG; u++) {
-        const int r = r0 + u;
-        v[u] = (live && r < rows) ? in[base + (long)r * row_stride + q] : make_double2(0.0, 0.0);
+    // ---- factors of this thread's rows, kept in registers for the whole chunk
+    double2 sub_c = zero, sup_c = zero;
+    if constexpr (CONST_ROWS) {
+        sub_c = shifted(subt, prow, 0, m0, m1, m2);
+        sup_c = shifted(supt, prow, 0, m0, m1, m2);
     }
-
-    // ---- compact right-hand-side operator in the transformed basis
-    if constexpr (SRC == 2) {
+    const double2 ui_in = (live && r0 > 0 && r0 < rows) ? Pv[(long)L.s * lines + q] : zero; // 1/P of row r0-1
+    double2 ui[kSeg];
+    double2 Af = one, Ab = one;
+    {
+        double2 uprev = ui_in;
+        const double2 dia_c = CONST_ROWS ? shifted(diagt, prow, 0, m0, m1, m2) : zero;
 #pragma unroll
-        for (int u = 0; u < SEG; u++) v[u] = cscale(v[u], sp.h2);
-    } else if constexpr (SRC == 4 || SRC == 6) {
-        double2 alpha;
-        double  beta;
-        if constexpr (SRC == 4) {
-            alpha = make_double2(sp.dim == 2 ? (10.0 + m1) / 12.0 : (8.0 + m1 + m2) / 12.0, 0.0);
-            beta = 1.0 / 12.0;
-        } else {
-            if (sp.dim == 2) {
-                const double muq = 12.0 * (m1 - 2.0) / (10.0 + m1);
-                alpha = make_double2(1.0 + muq / 12.0 + (m1 - 2.0) * muq / 360.0 - sp.k2h2_20.x, -sp.k2h2_20.y);
-                beta = muq / 90.0;
-            } else {
-                const double mx = 12.0 * (m1 - 2.0) / (10.0 + m1), my = 12.0 * (m2 - 2.0) / (10.0 + m2);
-                alpha = make_double2(1.0 + (mx + my) / 12.0 + ((m1 - 2.0) * mx + (m2 - 2.0) * my) / 360.0 +
-                                         (m2 - 2.0) * mx / 90.0 - sp.k2h2_20.x,
-                                     -sp.k2h2_20.y);
-                beta = (mx + my) / 90.0;
-            }
-        }
-        double2 before, after;
-        segment_neighbours<SEG>(v, c, s, CW, P, sA, sB, before, after);
-        double2 d[SEG];
-#pragma unroll
-        for (int u = 0; u < SEG; u++) {
-            const double2 lo = (u == 0) ? before : v[u - 1];
-            const double2 hi = (u == SEG - 1) ? after : v[u + 1];
-            d[u] = make_double2(lo.x - 2.0 * v[u].x + hi.x, lo.y - 2.0 * v[u].y + hi.y);
-        }
-#pragma unroll
-        for (int u = 0; u < SEG; u++)
-            v[u] = make_double2(alpha.x * v[u].x - alpha.y * v[u].y + beta * d[u].x,
-                                alpha.x * v[u].y + alpha.y * v[u].x + beta * d[u].y);
-        if constexpr (SRC == 6) {
-            // omega = T^-1 (12 D2 g): Pade solve along the line (real constant factors)
-            double2 zh = make_double2(0.0, 0.0), A = make_double2(1.0, 0.0);
-#pragma unroll
-            for (int u = 0; u < SEG; u++) {
-                const int r = r0 + u;
-                if (r < rows) {
-                    const double l = __ldg(sp.pl + r);
-                    zh = make_double2(12.0 * d[u].x - l * zh.x, 12.0 * d[u].y - l * zh.y);
-                    A = make_double2(-l * A.x, -l * A.y);
-                }
-            }
-            double2 z = segment_scan<true>(A, zh, c, s, CW, P, sA, sB);
-#pragma unroll
-            for (int u = 0; u < SEG; u++) {
-                const int r = r0 + u;
-                if (r < rows) {
-                    const double l = __ldg(sp.pl + r);
-                    z = make_double2(12.0 * d[u].x - l * z.x, 12.0 * d[u].y - l * z.y);
-                    d[u] = z;
-                }
-            }
-            double2 wh = make_double2(0.0, 0.0);
-            A = make_double2(1.0, 0.0);
-#pragma unroll
-            for (int u = SEG - 1; u >= 0; u--) {
-                const int r = r0 + u;
-                if (r < rows) {
-                    const double iu = __ldg(sp.pu + r);
-                    wh = make_double2((d[u].x - wh.x) * iu, (d[u].y - wh.y) * iu);
-                    A = make_double2(-iu * A.x, -iu * A.y);
-                }
-            }
-            double2 w = segment_scan<false>(A, wh, c, s, CW, P, sA, sB);
-#pragma unroll
-            for (int u = SEG - 1; u >= 0; u--) {
-                const int r = r0 + u;
-                if (r < rows) {
-                    const double iu = __ldg(sp.pu + r);
-                    w = make_double2((d[u].x - w.x) * iu, (d[u].y - w.y) * iu);
-                    d[u] = w;
+        for (int u = 0; u < kSeg; u++) {
+            const int r = r0 + u;
+            double2   Lr = zero;
+            ui[u] = zero;
+            if (live && r < rows) {
+                const double2 dia = CONST_ROWS ? dia_c : shifted(diagt, prow, r, m0, m1, m2);
+                if (r == 0) {
+                    ui[u] = first_pivot(dia);
                 } else {
-                    d[u] = make_double2(0.0, 0.0);
+                    const double2 sb = CONST_ROWS ? sub_c : shifted(subt, prow, r, m0, m1, m2);
+                    const double2 sp_ = CONST_ROWS ? sup_c : shifted(supt, prow, r - 1, m0, m1, m2);
+                    ui[u] = factor_step(sb, dia, sp_, uprev, Lr);
                 }
+            } else if (live && r > 0 && u > 0) {
+                const double2 sb = CONST_ROWS ? sub_c : shifted(subt, prow, r, m0, m1, m2);
+                Lr = cmul(sb, uprev); // first padded row: L is still formed from the last real pivot
             }
-            segment_neighbours<SEG>(d, c, s, CW, P, sA, sB, before, after);
-#pragma unroll
-            for (int u = 0; u < SEG; u++) {
-                const double2 lo = (u == 0) ? before : d[u - 1];
-                const double2 hi = (u == SEG - 1) ? after : d[u + 1];
-                const double2 d2w = make_double2(lo.x - 2.0 * d[u].x + hi.x, lo.y - 2.0 * d[u].y + hi.y);
-                v[u] = make_double2(v[u].x + d[u].x / 12.0 + d2w.x / 360.0, v[u].y + d[u].y / 12.0 + d2w.y / 360.0);
-            }
+            uprev = ui[u];
+            Af = cmul(Af, make_double2(-Lr.x, -Lr.y));
+            const double2 sp2 = CONST_ROWS ? sup_c : shifted(supt, prow, r, m0, m1, m2);
+            const double2 tau = cmul(sp2, ui[u]);
+            Ab = cmul(Ab, make_double2(-tau.x, -tau.y));
         }
-#pragma unroll
-        for (int u = 0; u < SEG; u++) v[u] = (r0 + u < rows) ? cscale(v[u], sp.h2) : make_double2(0.0, 0.0);
     }
 
-    // ---- forward substitution y_r = f_r - L_r y_{r-1}
-    double2 yh = make_double2(0.0, 0.0), A = make_double2(1.0, 0.0);
-#pragma unroll
-    for (int u = 0; u < SEG; u++) {
-        const int r = r0 + u;
-        if (live && r < rows) {
-            const double2 L = __ldg(Lf + (long)r * lines + q);
-            yh = cfms(v[u], L, yh);
-            A = make_double2(-(L.x * A.x - L.y * A.y), -(L.x * A.y + L.y * A.x));
+    // per-line coefficients of the compact right-hand-side operator
+    double2 alpha = one;
+    double  beta = 0.0;
+    if constexpr (SRC == 4) {
+        alpha = make_double2(sp.dim == 2 ? (10.0 + m1) / 12.0 : (8.0 + m1 + m2) / 12.0, 0.0);
+        beta = 1.0 / 12.0;
+    } else if constexpr (SRC == 6) {
+        if (sp.dim == 2) {
+            const double muq = 12.0 * (m1 - 2.0) / (10.0 + m1);
+            alpha = make_double2(1.6 + muq / 12.0 + (m1 - 2.0) * muq / 360.0 - sp.k2h2_20.x, -sp.k2h2_20.y);
+            beta = muq / 90.0 + 1.0 / 30.0;
+        } else {
+            const double mx = 12.0 * (m1 - 2.0) / (10.0 + m1), my = 12.0 * (m2 - 2.0) / (10.0 + m2);
+            alpha = make_double2(1.6 + (mx + my) / 12.0 + ((m1 - 2.0) * mx + (m2 - 2.0) * my) / 360.0 +
+                                     (m2 - 2.0) * mx / 90.0 - sp.k2h2_20.x,
+                                 -sp.k2h2_20.y);
+            beta = (mx + my) / 90.0 + 1.0 / 30.0;
         }
     }
-    double2 y = segment_scan<true>(A, yh, c, s, CW, P, sA, sB);
+    const double *pl = sp.pl + r0, *pu = sp.pu + r0; // this segment's Pade factors (L1-resident)
+    double pa = 1.0, pb = 1.0;                           // Pade segment products
+    if constexpr (SRC == 6) {
 #pragma unroll
-    for (int u = 0; u < SEG; u++) {
-        const int r = r0 + u;
-        if (live && r < rows) {
-            const double2 L = __ldg(Lf + (long)r * lines + q);
-            y = cfms(v[u], L, y);
+        for (int u = 0; u < kSeg; u++) {
+            pa *= -__ldg(pl + u);
+            pb *= -__ldg(pu + u);
+        }
+    }
+
+    const int  b_begin = blockIdx.y * rb;
+    const int  b_end = min(batch, b_begin + rb);
+    const long off0 = (long)r0 * row_stride + qq;
+    auto prefetch = [&](int b) {
+        const double2 *src = in + (long)b * field + off0;
+#pragma unroll
+        for (int u = 0; u < kSeg; u++) {
+            const bool ok = live && r0 + u < rows;
+            cp_async16(&pre[u * kLineThreads + threadIdx.x], ok ? src + (long)u * row_stride : in, ok ? 16 : 0);
+        }
+        cp_async_commit();
+    };
+    prefetch(b_begin);
+    int par = 0;
+    for (int b = b_begin; b < b_end; b++) {
+        double2 v[kSeg];
+        cp_async_wait_all();
+#pragma unroll
+        for (int u = 0; u < kSeg; u++) v[u] = pre[u * kLineThreads + threadIdx.x];
+        if (b + 1 < b_end) prefetch(b + 1);
+
+        // ---- compact right-hand-side operator in the transformed basis
+        if constexpr (SRC == 2) {
+#pragma unroll
+            for (int u = 0; u < kSeg; u++) v[u] = cscale(v[u], sp.h2);
+        } else if constexpr (SRC == 4 || SRC == 6) {
+            double2 before, after;
+            neighbours(v[0], v[kSeg - 1], L, sm, par, before, after);
+            par ^= 1;
+            double2 zh = zero;
+            if constexpr (SRC == 6) {
+                // forward Pade sweep of g (local part): z_r = g_r - l_r z_{r-1}
+#pragma unroll
+                for (int u = 0; u < kSeg; u++) {
+                    const double l = __ldg(pl + u);
+                    zh = make_double2(v[u].x - l * zh.x, v[u].y - l * zh.y);
+                    wsm[u * kLineThreads] = zh;
+                }
+            }
+            double2 gprev = before;
+#pragma unroll
+            for (int u = 0; u < kSeg; u++) {
+                const double2 g = v[u];
+                const double2 hi = (u == kSeg - 1) ? after : v[u + 1];
+                const double2 d2 = make_double2(gprev.x - 2.0 * g.x + hi.x, gprev.y - 2.0 * g.y + hi.y);
+                gprev = g;
+                v[u] = make_double2(fma(alpha.x, g.x, fma(-alpha.y, g.y, beta * d2.x)),
+                                    fma(alpha.x, g.y, fma(alpha.y, g.x, beta * d2.y)));
+            }
+            if constexpr (SRC == 6) {
+                // complete the forward sweep from the exact entering value, then the backward one:
+                // w_r = (z_r - w_{r+1}) / U_r;  F += -7.2 w
+                const double2 zin = scan_forward(make_double2(pa, 0.0), zh, L, sm, par);
+                par ^= 1;
+                double2 corr = zin;
+#pragma unroll
+                for (int u = 0; u < kSeg; u++) {
+                    const double l = __ldg(pl + u);
+                    corr = make_double2(-l * corr.x, -l * corr.y);
+                    const double2 z = wsm[u * kLineThreads];
+                    wsm[u * kLineThreads] = make_double2(z.x + corr.x, z.y + corr.y);
+                }
+                double2 wh = zero;
+#pragma unroll
+                for (int u = kSeg - 1; u >= 0; u--) {
+                    const double  iu = __ldg(pu + u);
+                    const double2 z = wsm[u * kLineThreads];
+                    wh = make_double2((z.x - wh.x) * iu, (z.y - wh.y) * iu);
+                }
+                const double2 win = scan_backward(make_double2(pb, 0.0), wh, L, sm, par);
+                par ^= 1;
+                double2 wv = win;
+#pragma unroll
+                for (int u = kSeg - 1; u >= 0; u--) {
+                    const double  iu = __ldg(pu + u);
+                    const double2 z = wsm[u * kLineThreads];
+                    wv = make_double2((z.x - wv.x) * iu, (z.y - wv.y) * iu);
+                    v[u] = make_double2(fma(-7.2, wv.x, v[u].x), fma(-7.2, wv.y, v[u].y));
+                }
+            }
+        }
+        if constexpr (SRC == 4 || SRC == 6) {
+#pragma unroll
+            for (int u = 0; u < kSeg; u++) v[u] = cscale(v[u], sp.h2);
+        }
+
+        // ---- forward substitution y_r = f_r - L_r y_{r-1},  L_r = sub_r / P_{r-1}
+        double2 yh = zero;
+#pragma unroll
+        for (int u = 0; u < kSeg; u++) {
+            const double2 sb = CONST_ROWS ? sub_c : shifted(subt, prow, r0 + u, m0, m1, m2);
+            yh = cfms(v[u], cmul(sb, u == 0 ? ui_in : ui[u - 1]), yh);
+        }
+        double2 y = scan_forward(Af, yh, L, sm, par);
+        par ^= 1;
+#pragma unroll
+        for (int u = 0; u < kSeg; u++) {
+            const double2 sb = CONST_ROWS ? sub_c : shifted(subt, prow, r0 + u, m0, m1, m2);
+            y = cfms(v[u], cmul(sb, u == 0 ? ui_in : ui[u - 1]), y);
             v[u] = y;
         }
-    }
 
-    // ---- back substitution x_r = y_r/P_r - (super_r/P_r) x_{r+1}
-    double2 xh = make_double2(0.0, 0.0);
-    A = make_double2(1.0, 0.0);
+        // ---- back substitution x_r = (y_r - super_r x_{r+1}) / P_r
+        double2 xh = zero;
 #pragma unroll
-    for (int u = SEG - 1; u >= 0; u--) {
-        const int r = r0 + u;
-        if (live && r < rows) {
-            const double2 ui = __ldg(Ui + (long)r * lines + q);
-            const double2 tau = cmul(shifted(supt, rows, r, m0, m1, m2), ui); // super_r / P_r
-            xh = cfms(cmul(v[u], ui), tau, xh);
-            A = make_double2(-(tau.x * A.x - tau.y * A.y), -(tau.x * A.y + tau.y * A.x));
+        for (int u = kSeg - 1; u >= 0; u--) {
+            const double2 sp2 = CONST_ROWS ? sup_c : shifted(supt, prow, r0 + u, m0, m1, m2);
+            xh = cmul(cfms(v[u], sp2, xh), ui[u]);
         }
-    }
-    double2 x = segment_scan<false>(A, xh, c, s, CW, P, sA, sB);
+        double2 x = scan_backward(Ab, xh, L, sm, par);
+        par ^= 1;
 #pragma unroll
-    for (int u = SEG - 1; u >= 0; u--) {
-        const int r = r0 + u;
-        if (live && r < rows) {
-            const double2 ui = __ldg(Ui + (long)r * lines + q);
-            const double2 tau = cmul(shifted(supt, rows, r, m0, m1, m2), ui);
-            x = cfms(cmul(v[u], ui), tau, x);
+        for (int u = kSeg - 1; u >= 0; u--) {
+            const double2 sp2 = CONST_ROWS ? sup_c : shifted(supt, prow, r0 + u, m0, m1, m2);
+            x = cmul(cfms(v[u], sp2, x), ui[u]);
             v[u] = x;
         }
-    }
 
+        double2 *dst = out + (long)b * field + off0;
 #pragma unroll
-    for (int u = 0; u < SEG; u++) {
-        const int r = r0 + u;
-        if (live && r < rows) out[base + (long)r * row_stride + q] = v[u];
+        for (int u = 0; u < kSeg; u++)
+            if (live && r0 + u < rows) dst[(long)u * row_stride] = v[u];
     }
 }
 
-static int solve_geometry(int rows, int seg, int *CW, int *P) {
-    int p = 1;
-    while (p * seg < rows) p <<= 1;
-    if (p > kSolveThreads) {
-        set_error("line length %d exceeds %d", rows, kSolveThreads * seg);
+// segments per line: a power of two >= kMinSegments (so at most 32 lines share a warp)
+static int solve_geometry(int rows, int *CW, int *P) {
+    int p = kMinSegments;
+    while (p * kSeg < rows) p <<= 1;
+    if (p > kLineThreads) {
+        set_error("line length %d exceeds %d", rows, kLineThreads * kSeg);
         return HH_ERR_UNSUPPORTED;
     }
     *P = p;
-    *CW = kSolveThreads / p;
+    *CW = kLineThreads / p;
     return HH_OK;
 }
 
-template <int SEG, int SRC> static int launch_solve_t(Plan *p, const double2 *in, double2 *out, int batch) {
+int padded_rows(int rows) {
     int CW, P;
-    HH_TRY(solve_geometry(p->rows, SEG, &CW, &P));
+    if (solve_geometry(rows, &CW, &P) != HH_OK) return rows;
+    return P * kSeg;
+}
+
+template <int SRC, bool CR> static int launch_solve_t(Plan *p, const double2 *in, double2 *out, int batch) {
+    int CW, P;
+    HH_TRY(solve_geometry(p->rows, &CW, &P));
     SrcParams sp;
     sp.dim = p->dim;
     sp.h2 = p->h * p->h;
     sp.k2h2_20 = make_double2(p->k2.x * sp.h2 / 20.0, p->k2.y * sp.h2 / 20.0);
     sp.pl = p->pade_l;
     sp.pu = p->pade_u;
-    dim3 grid((unsigned)((p->lines + CW - 1) / CW), (unsigned)batch);
-    k_line_solve<SEG, SRC><<<grid, kSolveThreads, 0, p->ctx->stream>>>(in, out, p->lines, p->rows, p->row_stride,
-                                                                         p->field, CW, P, p->Lf, p->Ui, p->rowc, p->mu,
-                                                                         sp);
+    const int shm = (int)(sizeof(double2) * kSeg * kLineThreads) * (SRC == 6 ? 2 : 1);
+    HH_CUDA(cudaFuncSetAttribute(k_line_solve<SRC, CR>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
+    // right-hand sides per CTA: enough CTAs to fill the SMs twice, factors reused within a chunk
+    const long groups = (p->lines + CW - 1) / CW;
+    int rb = 1;
+    while (rb < batch && groups * ((batch + 2 * rb - 1) / (2 * rb)) >= 2L * 148) rb *= 2;
+    const int chunks = (batch + rb - 1) / rb;
+    dim3 grid((unsigned)groups, (unsigned)chunks);
+    k_line_solve<SRC, CR><<<grid, kLineThreads, shm, p->ctx->stream>>>(in, out, p->lines, p->rows, p->prow,
+                                                                         p->row_stride, p->field, batch, rb, CW, p->Pv,
+                                                                         p->subt, p->diagt, p->rowc, p->mu, sp);
     HH_CUDA(cudaGetLastError());
     p->ctx->launches++;
     return HH_OK;
 }
 
-int launch_line_solve(Plan *p, const double2 *in, double2 *out, int batch, int src_order) {
-    switch (src_order) {
-    case 0: return launch_solve_t<16, 0>(p, in, out, batch);
-    case 2: return launch_solve_t<16, 2>(p, in, out, batch);
-    case 4: return launch_solve_t<16, 4>(p, in, out, batch);
-    case 6: return launch_solve_t<8, 6>(p, in, out, batch);
-    default: set_error("source operator order %d", src_order); return HH_ERR_INVALID;
+template <bool CR> static int launch_solve_cr(Plan *p, const double2 *in, double2 *out, int batch, int src) {
+    switch (src) {
+    case 0: return launch_solve_t<0, CR>(p, in, out, batch);
+    case 2: return launch_solve_t<2, CR>(p, in, out, batch);
+    case 4: return launch_solve_t<4, CR>(p, in, out, batch);
+    case 6: return launch_solve_t<6, CR>(p, in, out, batch);
+    default: set_error("source operator order %d", src); return HH_ERR_INVALID;
     }
 }
+
+int launch_line_solve(Plan *p, const double2 *in, double2 *out, int batch, int src_order) {
+    if (src_order == 6 && !p->pade_l) {
+        set_error("order-6 source operator needs a Helmholtz plan");
+        return HH_ERR_INVALID;
+    }
+    return p->const_rows ? launch_solve_cr<true>(p, in, out, batch, src_order)
+                         : launch_solve_cr<false>(p, in, out, batch, src_order);
+}
+
+int segment_count(int rows) { return (rows + kSeg - 1) / kSeg; }
 
 } // namespace hh

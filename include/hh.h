@@ -45,6 +45,8 @@ int         hh_version(void);                 /* major*10000 + minor*100 + patch
 /* --------------------------------------------------------------- contexts ---- */
 /* stream: a cudaStream_t to launch on, or NULL for a context-owned stream. */
 int hh_ctx_create(int device, void *stream, hh_ctx **out);
+/* Destroys the context together with every plan still alive on it (those plan handles become
+ * invalid).  To launch on the legacy default stream pass cudaStreamLegacy ((void *)1). */
 int hh_ctx_destroy(hh_ctx *ctx);
 int hh_ctx_set_stream(hh_ctx *ctx, void *stream);
 int hh_ctx_synchronize(hh_ctx *ctx);          /* also surfaces kernel-reported failures   */

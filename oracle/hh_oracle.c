@@ -695,3 +695,52 @@ void ora_residual_3d(int nx, int ny, int nz, const ora_coef3d *c, const cplx *so
     for (long t = 0; t < nxy * nz; t++) res[t] = res[t] - rhs[t];
     free(e);
 }
+
+/* ============================================================ extended precision ====== */
+/* The 2D solve with the per-mode Thomas factorisation and substitutions carried out in long
+ * double (x87 80-bit) instead of double; the two DSTs stay in double (their rounding is at the
+ * 1e-16 level and is not amplified).  It restates solver.c:71-86 and LU.c:12-40 in higher
+ * precision so tests can measure how far the reference's own double result is from the exact
+ * solution of its discrete system on ill-conditioned (near-resonant) lines. */
+int ora_solver_2d_ld(int nx, int ny, const ora_coef2d *c, const cplx *rhs, cplx *sol) {
+    typedef long double _Complex lcplx;
+    const long nxy = (long)nx * ny;
+    cplx  *rhat = (cplx *)malloc(sizeof(cplx) * (size_t)nxy);
+    cplx  *xhat = (cplx *)malloc(sizeof(cplx) * (size_t)nxy);
+    cplx  *rowt = (cplx *)malloc(sizeof(cplx) * (size_t)nx);
+    lcplx *U = (lcplx *)malloc(sizeof(lcplx) * (size_t)ny);
+    lcplx *y = (lcplx *)malloc(sizeof(lcplx) * (size_t)ny);
+    if (!rhat || !xhat || !rowt || !U || !y) return -1;
+    if (ora_dst1_rows(nx, ny, rhs, nx, rhat, nx) != 0) return -1;
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int i = 0; i < nx; i++) {
+        const long double ex = 2.0L * cosl((i + 1) * pi / (nx + 1));
+        lcplx sup_prev = 0;
+        for (int j = 0; j < ny; j++) {
+            const lcplx sub = (lcplx)c->bm[j] * ex + (lcplx)c->am[j];
+            const lcplx dia = (lcplx)c->b[j] * ex + (lcplx)c->a[j];
+            if (j == 0) {
+                U[0] = dia;
+                y[0] = rhat[i];
+            } else {
+                const lcplx L = sub / U[j - 1];
+                U[j] = dia - L * sup_prev;
+                y[j] = (lcplx)rhat[i + (long)j * nx] - L * y[j - 1];
+            }
+            sup_prev = (lcplx)c->bp[j] * ex + (lcplx)c->ap[j];
+        }
+        lcplx x = y[ny - 1] / U[ny - 1];
+        xhat[ny - 1 + (long)i * ny] = (cplx)x;
+        for (int j = ny - 2; j >= 0; j--) {
+            const lcplx sup = (lcplx)c->bp[j] * ex + (lcplx)c->ap[j];
+            x = (y[j] - sup * x) / U[j];
+            xhat[j + (long)i * ny] = (cplx)x;
+        }
+    }
+    for (int j = 0; j < ny; j++) {
+        for (int i = 0; i < nx; i++) rowt[i] = xhat[j + (long)i * ny];
+        if (ora_dst1_rows(nx, 1, rowt, nx, sol + (long)j * nx, nx) != 0) return -1;
+    }
+    free(rhat); free(xhat); free(rowt); free(U); free(y);
+    return 0;
+}

@@ -69,6 +69,10 @@ void ora_lu_2d(int nx, int ny, const ora_coef2d *c, ora_cplx *L, ora_cplx *U, or
 /* 2D_Program/solver_functions/solver.c:14-117 (forward DST, per-mode Thomas, inverse). */
 int  ora_solver_2d(int nx, int ny, const ora_cplx *rhs, const ora_cplx *L, const ora_cplx *U,
                    const ora_cplx *Up, ora_cplx *sol);
+/* solver.c:14-117 with the per-mode Thomas solves in long double: the exact solution of the
+ * discrete system to ~1e-18 relative per line, for measuring rounding error on ill-conditioned
+ * (near-resonant) lines.  Factors are formed from the stencil rows as LU.c:12-40 does. */
+int  ora_solver_2d_ld(int nx, int ny, const ora_coef2d *c, const ora_cplx *rhs, ora_cplx *sol);
 /* 2D_Program/main_functions/residual.c:3-34: res = A*sol - rhs (zero Dirichlet ring). */
 void ora_residual_2d(int nx, int ny, const ora_coef2d *c, const ora_cplx *sol, const ora_cplx *rhs,
                      ora_cplx *res);

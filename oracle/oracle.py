@@ -125,6 +125,16 @@ class Oracle:
         assert rc == 0
         return sol
 
+    def solver_2d_ld(self, co, rhs) -> np.ndarray:
+        """Extended-precision solve of the same discrete system (see ora_solver_2d_ld)."""
+        ny, nx = rhs.shape
+        rhs = np.ascontiguousarray(rhs)
+        sol = np.zeros_like(rhs)
+        cs = self._cs2(co)
+        rc = self.lib.ora_solver_2d_ld(C.c_int(nx), C.c_int(ny), C.byref(cs), _ptr(rhs), _ptr(sol))
+        assert rc == 0
+        return sol
+
     def residual_2d(self, co, sol, rhs) -> np.ndarray:
         ny, nx = sol.shape
         res = np.zeros_like(sol)

@@ -193,3 +193,17 @@ def test_restatement_matches_live_reference(oracle):
     f = W.source_2d(n, W.sine_modes(77, 8, 10), noise_seed=78, noise_var=1e-3)
     run = Reference2D().pipeline(n, order, k, f, threads=2)
     assert np.array_equal(oracle.pipeline_2d(n, order, k, f)["sol"], run.arrays["sol"].reshape(n, n))
+
+
+def test_extended_precision_solver_bounds_reference_error(oracle):
+    """The long-double solve is the exact discrete solution to far below FP64 rounding: on a
+    well-conditioned case the reference agrees with it to ~1e-15, and on the near-resonant
+    k=10 case (k^2 - 10 pi^2 = 1.3) the reference's own rounding error is visible."""
+    n = 63
+    f = W.source_2d(n, W.sine_modes(5, 8, 20), noise_seed=6, noise_var=1e-3)
+    ref = oracle.pipeline_2d(n, 6, 50.0, f)
+    truth = oracle.solver_2d_ld(ref["coef"], ref["rhs"])
+    assert rel_err(ref["sol"], truth) < 1e-13
+    ref = oracle.pipeline_2d(n, 4, 10.0, f)
+    truth = oracle.solver_2d_ld(ref["coef"], ref["rhs"])
+    assert rel_err(ref["sol"], truth) < 1e-11
