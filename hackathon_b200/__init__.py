@@ -46,6 +46,9 @@ SIGNATURES = {
     "hh_plan3d_create_helmholtz": (_i, [_vp, _i, _i, _d, _d, C.POINTER(_vp)]),
     "hh_plan_destroy": (_i, [_vp]),
     "hh_plan_field_size": (_l, [_vp]),
+    "hh_plan_tune": (_i, [_vp, _i]),
+    "hh_plan_set_variant": (_i, [_vp, _i]),
+    "hh_plan_variant": (_i, [_vp]),
     "hh_solve": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_host": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source": (_i, [_vp, _vp, _vp, _i]),
@@ -199,6 +202,19 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+    def tune(self, batch: int) -> int:
+        """Time the line-solve variants on `batch` right-hand sides, keep the fastest."""
+        check(lib().hh_plan_tune(self.h, batch), "hh_plan_tune")
+        return self.variant
+
+    @property
+    def variant(self) -> int:
+        return int(lib().hh_plan_variant(self.h))
+
+    @variant.setter
+    def variant(self, v: int):
+        check(lib().hh_plan_set_variant(self.h, v), "hh_plan_set_variant")
 
     # -- device buffers (torch tensors / raw addresses)
     def solve(self, rhs, sol, batch: int = 1):

@@ -280,6 +280,22 @@ static int plan_pade(hh_plan *pl) {
         U = 10.0 - L[r];
         Ui[r] = 1.0 / U;
     }
+    // the kernel replaces rows >= 9 by the limit; it is an exact fixed point in double
+    {
+        double u = 10.0, lim_l = 0.0, lim_u = 0.0;
+        for (int r = 1; r < 64; r++) {
+            lim_l = 1.0 / u;
+            u = 10.0 - lim_l;
+            lim_u = 1.0 / u;
+        }
+        p.pade_linf = lim_l;
+        p.pade_uinf = lim_u;
+        for (int r = 9; r < p.rows; r++)
+            if (L[r] != lim_l || Ui[r] != lim_u) {
+                set_error("Pade factors not converged at row %d", r);
+                return HH_ERR_UNSUPPORTED;
+            }
+    }
     HH_CUDA(cudaMalloc(&p.pade_l, sizeof(double) * (size_t)p.prow));
     HH_CUDA(cudaMalloc(&p.pade_u, sizeof(double) * (size_t)p.prow));
     HH_CUDA(cudaMemcpy(p.pade_l, L.data(), sizeof(double) * (size_t)p.prow, cudaMemcpyHostToDevice));
@@ -454,6 +470,67 @@ extern "C" int hh_plan_destroy(hh_plan *pl) {
 }
 
 extern "C" long hh_plan_field_size(const hh_plan *pl) { return pl ? pl->p.field : 0; }
+
+static int check_batch(hh_plan *pl, int batch);
+
+extern "C" int hh_plan_set_variant(hh_plan *pl, int variant) {
+    if (!pl || variant < 0 || variant >= solve_variant_count()) {
+        set_error("invalid plan or line-solve variant %d", variant);
+        return HH_ERR_INVALID;
+    }
+    pl->p.variant = variant;
+    return HH_OK;
+}
+
+extern "C" int hh_plan_variant(const hh_plan *pl) { return pl ? pl->p.variant : -1; }
+
+// Times every line-solve variant on `batch` zero right-hand sides (the solve does the same work
+// for any values) and keeps the fastest.  Blocks; must not run inside a stream capture.
+extern "C" int hh_plan_tune(hh_plan *pl, int batch) {
+    HH_TRY(check_batch(pl, batch));
+    if (batch == 0) return HH_OK;
+    Plan &p = pl->p;
+    Ctx  *c = p.ctx;
+    HH_CUDA(cudaSetDevice(c->device));
+    double2 *buf = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = HH_OK, best = p.variant;
+    float best_ms = 1e30f;
+    const int src = p.src_order;
+    auto run = [&]() -> int {
+        if (cudaMalloc(&buf, sizeof(double2) * (size_t)p.field * batch) != cudaSuccess ||
+            cudaMemsetAsync(buf, 0, sizeof(double2) * (size_t)p.field * batch, c->stream) != cudaSuccess ||
+            cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+            set_error("hh_plan_tune: %s", cudaGetErrorString(cudaGetLastError()));
+            return HH_ERR_CUDA;
+        }
+        for (int v = 0; v < solve_variant_count(); v++) {
+            p.variant = v;
+            HH_TRY(launch_line_solve(&p, buf, buf, batch, src)); // warm-up
+            HH_CUDA(cudaEventRecord(e0, c->stream));
+            for (int r = 0; r < 3; r++) HH_TRY(launch_line_solve(&p, buf, buf, batch, src));
+            HH_CUDA(cudaEventRecord(e1, c->stream));
+            HH_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            HH_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = v;
+            }
+        }
+        return HH_OK;
+    };
+    rc = run();
+    p.variant = best;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (buf) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(buf);
+    }
+    if (rc == HH_OK) rc = hh_ctx_synchronize(reinterpret_cast<hh_ctx *>(c)); // Ctx is hh_ctx's first member
+    return rc;
+}
 
 // -------------------------------------------------------------------- solve ------
 static int transform_forward(Plan &p, const double2 *in, double2 *out, int batch) {

@@ -98,6 +98,7 @@ struct Plan {
     // reciprocal Thomas pivot of the row before each 16-row segment, [segment][line]
     double2 *Pv = nullptr;
     bool     const_rows = false; // stencil row tables constant along the line
+    int      variant = 0;        // line-solve thread mapping (see solve_variant_count / autotune)
     double2 *subt = nullptr, *diagt = nullptr; // sub/diagonal row tables (4 * rows each)
     // super-diagonal(row, line) = rowc[0][row] mu[0][line] + rowc[1][row] mu[1][line] + rowc[2][row] mu[2][line] + rowc[3][row]
     double2 *rowc = nullptr;        // 4 * rows complex
@@ -105,6 +106,7 @@ struct Plan {
     // fused source operator (homogeneous Dirichlet, constant k): 0 = off
     int      src_order = 0;
     double  *pade_l = nullptr, *pade_u = nullptr; // [1 10 1] factors along the line (rows each)
+    double   pade_linf = 0.0, pade_uinf = 0.0;     // their common limit (reached from row 9 on)
     double   h = 0.0;
     double2  k2 = {0.0, 0.0};
 };
@@ -117,6 +119,7 @@ int launch_line_solve(Plan *p, const double2 *in, double2 *out, int batch, int s
 int read_device_error(Ctx *c, int *val);
 int segment_count(int rows);
 int padded_rows(int rows);
+int solve_variant_count();
 
 
 } // namespace hh

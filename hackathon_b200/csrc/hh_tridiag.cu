@@ -67,9 +67,6 @@ __device__ __forceinline__ double2 shifted(const double2 *__restrict__ tab, int 
 
 // ----------------------------------------------------------------- factors --------
 constexpr int kSeg = 8;          // rows per thread in the solve
-constexpr int kLineThreads = 512;
-constexpr int kWarps = kLineThreads / 32;
-constexpr int kMinSegments = 16; // at most 32 lines per CTA
 
 // One step of the factor recurrence, shared by the set-up and the solve so both produce the
 // same values: L = sub / P_prev (as sub * (1/P_prev)), P = diag - L super_prev, returns 1/P.
@@ -128,12 +125,54 @@ __device__ __forceinline__ double2 shfl_down2(double2 v, int off) {
     return make_double2(__shfl_down_sync(0xffffffffu, v.x, off), __shfl_down_sync(0xffffffffu, v.y, off));
 }
 
-struct ScanSmem {
-    double2 A[2][kWarps][32], B[2][kWarps][32]; // cross-warp totals / neighbour values (double buffered)
+template <int NW> struct ScanSmem {
+    double2 A[2][NW][32], B[2][NW][32]; // cross-warp totals / neighbour values (double buffered)
+    double2 E[NW][32];                  // value entering each warp's first segment, per line
+                                        // (rewritten only after the next scan's barrier)
+    double  pl[9], pu[9];               // Pade factors of rows 0..8 (constant from row 9 on)
 };
 
+// shuffles within groups of NW lanes (the warps of one line in cross_warp_scan)
+template <int NW> __device__ __forceinline__ double2 shfl_up_w(double2 v, int off) {
+    return make_double2(__shfl_up_sync(0xffffffffu, v.x, off, NW), __shfl_up_sync(0xffffffffu, v.y, off, NW));
+}
+template <int NW> __device__ __forceinline__ double2 shfl_down_w(double2 v, int off) {
+    return make_double2(__shfl_down_sync(0xffffffffu, v.x, off, NW), __shfl_down_sync(0xffffffffu, v.y, off, NW));
+}
+
+// Exclusive scan of the per-warp maps (sm.A, sm.B)[par][w][c] over w, for every line c of the CTA:
+// sm.E[w][c] = value entering warp w.  Thread t < NW*CW handles (w = t % NW, c = t / NW); the NW
+// warps of a line sit in consecutive lanes, so the scan is a width-NW shuffle scan.  FORWARD
+// composes warps left to right, else right to left.
+template <int NW, bool FORWARD>
+__device__ __forceinline__ void cross_warp_scan(ScanSmem<NW> &sm, int par, int CW) {
+    const int t = threadIdx.x;
+    if ((t >> 5) < (NW * CW + 31) / 32) { // whole warps take part in the shuffles
+        const bool in = t < NW * CW;
+        const int  w = t % NW, c = t / NW;
+        const int  pos = FORWARD ? w : NW - 1 - w;
+        double2 A = make_double2(1.0, 0.0), B = make_double2(0.0, 0.0);
+        if (in) {
+            A = sm.A[par][w][c];
+            B = sm.B[par][w][c];
+        }
+        for (int off = 1; off < NW; off <<= 1) {
+            const double2 Ao = FORWARD ? shfl_up_w<NW>(A, off) : shfl_down_w<NW>(A, off);
+            const double2 Bo = FORWARD ? shfl_up_w<NW>(B, off) : shfl_down_w<NW>(B, off);
+            if (pos >= off) {
+                B = cfma(B, A, Bo);
+                A = cmul(A, Ao);
+            }
+        }
+        double2 Ex = FORWARD ? shfl_up_w<NW>(B, 1) : shfl_down_w<NW>(B, 1);
+        if (pos == 0) Ex = make_double2(0.0, 0.0);
+        if (in) sm.E[w][c] = Ex;
+    }
+}
+
 // Value entering segment s for the left-to-right composition of maps (A, B): y = A y_in + B.
-__device__ __forceinline__ double2 scan_forward(double2 A, double2 B, const Lane &L, ScanSmem &sm, int par) {
+template <int NW>
+__device__ __forceinline__ double2 scan_forward(double2 A, double2 B, const Lane &L, ScanSmem<NW> &sm, int par) {
     for (int off = L.CW; off < 32; off <<= 1) {
         const double2 Al = shfl_up2(A, off), Bl = shfl_up2(B, off);
         if (L.lane >= off) {
@@ -145,13 +184,14 @@ __device__ __forceinline__ double2 scan_forward(double2 A, double2 B, const Lane
     if (L.sl == 0) { Ae = make_double2(1.0, 0.0); Be = make_double2(0.0, 0.0); }
     if (L.sl == L.SPW - 1) { sm.A[par][L.w][L.c] = A; sm.B[par][L.w][L.c] = B; }
     __syncthreads();
-    double2 E = make_double2(0.0, 0.0);
-    for (int w2 = 0; w2 < L.w; w2++) E = cfma(sm.B[par][w2][L.c], sm.A[par][w2][L.c], E);
-    return cfma(Be, Ae, E);
+    cross_warp_scan<NW, true>(sm, par, L.CW);
+    __syncthreads();
+    return cfma(Be, Ae, sm.E[L.w][L.c]);
 }
 
 // Value entering segment s from the right (maps composed right-to-left).
-__device__ __forceinline__ double2 scan_backward(double2 A, double2 B, const Lane &L, ScanSmem &sm, int par) {
+template <int NW>
+__device__ __forceinline__ double2 scan_backward(double2 A, double2 B, const Lane &L, ScanSmem<NW> &sm, int par) {
     for (int off = L.CW; off < 32; off <<= 1) {
         const double2 Ar = shfl_down2(A, off), Br = shfl_down2(B, off);
         if (L.lane + off < 32) {
@@ -163,13 +203,14 @@ __device__ __forceinline__ double2 scan_backward(double2 A, double2 B, const Lan
     if (L.sl == L.SPW - 1) { Ae = make_double2(1.0, 0.0); Be = make_double2(0.0, 0.0); }
     if (L.sl == 0) { sm.A[par][L.w][L.c] = A; sm.B[par][L.w][L.c] = B; }
     __syncthreads();
-    double2 E = make_double2(0.0, 0.0);
-    for (int w2 = kWarps - 1; w2 > L.w; w2--) E = cfma(sm.B[par][w2][L.c], sm.A[par][w2][L.c], E);
-    return cfma(Be, Ae, E);
+    cross_warp_scan<NW, false>(sm, par, L.CW);
+    __syncthreads();
+    return cfma(Be, Ae, sm.E[L.w][L.c]);
 }
 
 // Last value of segment s-1 and first value of segment s+1 (zero outside the line).
-__device__ __forceinline__ void neighbours(double2 lo, double2 hi, const Lane &L, ScanSmem &sm, int par,
+template <int NW>
+__device__ __forceinline__ void neighbours(double2 lo, double2 hi, const Lane &L, ScanSmem<NW> &sm, int par,
                                            double2 &prev_hi, double2 &next_lo) {
     prev_hi = shfl_up2(hi, L.CW);
     next_lo = shfl_down2(lo, L.CW);
@@ -177,7 +218,7 @@ __device__ __forceinline__ void neighbours(double2 lo, double2 hi, const Lane &L
     if (L.sl == 0) sm.A[par][L.w][L.c] = lo;
     __syncthreads();
     if (L.sl == 0) prev_hi = (L.w > 0) ? sm.B[par][L.w - 1][L.c] : make_double2(0.0, 0.0);
-    if (L.sl == L.SPW - 1) next_lo = (L.w < kWarps - 1) ? sm.A[par][L.w + 1][L.c] : make_double2(0.0, 0.0);
+    if (L.sl == L.SPW - 1) next_lo = (L.w < NW - 1) ? sm.A[par][L.w + 1][L.c] : make_double2(0.0, 0.0);
 }
 
 // 16-byte asynchronous global -> shared copy; src_bytes = 0 writes zeros.
@@ -196,23 +237,36 @@ struct SrcParams {
     double2 k2h2_20;  // k^2 h^2 / 20
     const double *pl; // Pade [1 10 1] multipliers L_r = 1/U_{r-1} (L_0 = 0); zero past the line
     const double *pu; // Pade reciprocal pivots 1/U_r; zero past the line
+    double linf, uinf;// both converge to 1/(5 + sqrt 24) exactly in double from row 9 on
 };
+
+// Pade factors of row r: rows 0..8 from shared memory, the fixed point up to the line end, zero
+// past it (neutral padded rows).
+template <int NW>
+__device__ __forceinline__ double pade_l(const ScanSmem<NW> &sm, const SrcParams &sp, int r, int rows) {
+    return r < 9 ? sm.pl[r] : (r < rows ? sp.linf : 0.0);
+}
+template <int NW>
+__device__ __forceinline__ double pade_u(const ScanSmem<NW> &sm, const SrcParams &sp, int r, int rows) {
+    return r < 9 ? sm.pu[r] : (r < rows ? sp.uinf : 0.0);
+}
 
 // SRC = 0: the input already is the transformed RHS.  SRC = 2/4/6: the input is the transformed
 // source g and the compact operator of that order is applied first (see the file header).
 // CONST_ROWS: the stencil rows do not vary along the line (constant k).
 // Rows past the end of a line are neutral: zero data, zero reciprocal pivots, zero Pade factors,
 // so the sweeps run without per-row conditions.
-template <int SRC, bool CONST_ROWS>
-__global__ void __launch_bounds__(kLineThreads, 1)
+template <int SRC, bool CONST_ROWS, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
     k_line_solve(const double2 *__restrict__ in, double2 *__restrict__ out, int lines, int rows, int prow,
                  long row_stride, long field, int batch, int rb, int CW, const double2 *__restrict__ Pv,
                  const double2 *__restrict__ subt, const double2 *__restrict__ diagt, const double2 *__restrict__ supt,
                  const double *__restrict__ mu, SrcParams sp) {
-    __shared__ ScanSmem sm;
-    extern __shared__ double2 pre[]; // [kSeg][kLineThreads] prefetch of the next right-hand side,
-                                     // then (SRC == 6) [kSeg][kLineThreads] Pade scratch
-    double2 *wsm = pre + kSeg * kLineThreads + threadIdx.x;
+    constexpr int NW = NT / 32;
+    __shared__ ScanSmem<NW> sm;
+    extern __shared__ double2 pre[]; // [kSeg][NT] prefetch of the next right-hand side,
+                                     // then (SRC == 6) [kSeg][NT] Pade scratch
+    double2 *wsm = pre + kSeg * NT + threadIdx.x;
     Lane L;
     L.lane = threadIdx.x & 31;
     L.w = threadIdx.x >> 5;
@@ -285,13 +339,17 @@ __global__ void __launch_bounds__(kLineThreads, 1)
             beta = (mx + my) / 90.0 + 1.0 / 30.0;
         }
     }
-    const double *pl = sp.pl + r0, *pu = sp.pu + r0; // this segment's Pade factors (L1-resident)
-    double pa = 1.0, pb = 1.0;                           // Pade segment products
+    double pa = 1.0, pb = 1.0; // Pade segment products
     if constexpr (SRC == 6) {
+        if (threadIdx.x < 9) {
+            sm.pl[threadIdx.x] = sp.pl[threadIdx.x];
+            sm.pu[threadIdx.x] = sp.pu[threadIdx.x];
+        }
+        __syncthreads();
 #pragma unroll
         for (int u = 0; u < kSeg; u++) {
-            pa *= -__ldg(pl + u);
-            pb *= -__ldg(pu + u);
+            pa *= -pade_l(sm, sp, r0 + u, rows);
+            pb *= -pade_u(sm, sp, r0 + u, rows);
         }
     }
 
@@ -303,7 +361,7 @@ __global__ void __launch_bounds__(kLineThreads, 1)
 #pragma unroll
         for (int u = 0; u < kSeg; u++) {
             const bool ok = live && r0 + u < rows;
-            cp_async16(&pre[u * kLineThreads + threadIdx.x], ok ? src + (long)u * row_stride : in, ok ? 16 : 0);
+            cp_async16(&pre[u * NT + threadIdx.x], ok ? src + (long)u * row_stride : in, ok ? 16 : 0);
         }
         cp_async_commit();
     };
@@ -313,7 +371,7 @@ __global__ void __launch_bounds__(kLineThreads, 1)
         double2 v[kSeg];
         cp_async_wait_all();
 #pragma unroll
-        for (int u = 0; u < kSeg; u++) v[u] = pre[u * kLineThreads + threadIdx.x];
+        for (int u = 0; u < kSeg; u++) v[u] = pre[u * NT + threadIdx.x];
         if (b + 1 < b_end) prefetch(b + 1);
 
         // ---- compact right-hand-side operator in the transformed basis
@@ -329,9 +387,9 @@ __global__ void __launch_bounds__(kLineThreads, 1)
                 // forward Pade sweep of g (local part): z_r = g_r - l_r z_{r-1}
 #pragma unroll
                 for (int u = 0; u < kSeg; u++) {
-                    const double l = __ldg(pl + u);
+                    const double l = pade_l(sm, sp, r0 + u, rows);
                     zh = make_double2(v[u].x - l * zh.x, v[u].y - l * zh.y);
-                    wsm[u * kLineThreads] = zh;
+                    wsm[u * NT] = zh;
                 }
             }
             double2 gprev = before;
@@ -352,16 +410,16 @@ __global__ void __launch_bounds__(kLineThreads, 1)
                 double2 corr = zin;
 #pragma unroll
                 for (int u = 0; u < kSeg; u++) {
-                    const double l = __ldg(pl + u);
+                    const double l = pade_l(sm, sp, r0 + u, rows);
                     corr = make_double2(-l * corr.x, -l * corr.y);
-                    const double2 z = wsm[u * kLineThreads];
-                    wsm[u * kLineThreads] = make_double2(z.x + corr.x, z.y + corr.y);
+                    const double2 z = wsm[u * NT];
+                    wsm[u * NT] = make_double2(z.x + corr.x, z.y + corr.y);
                 }
                 double2 wh = zero;
 #pragma unroll
                 for (int u = kSeg - 1; u >= 0; u--) {
-                    const double  iu = __ldg(pu + u);
-                    const double2 z = wsm[u * kLineThreads];
+                    const double  iu = pade_u(sm, sp, r0 + u, rows);
+                    const double2 z = wsm[u * NT];
                     wh = make_double2((z.x - wh.x) * iu, (z.y - wh.y) * iu);
                 }
                 const double2 win = scan_backward(make_double2(pb, 0.0), wh, L, sm, par);
@@ -369,8 +427,8 @@ __global__ void __launch_bounds__(kLineThreads, 1)
                 double2 wv = win;
 #pragma unroll
                 for (int u = kSeg - 1; u >= 0; u--) {
-                    const double  iu = __ldg(pu + u);
-                    const double2 z = wsm[u * kLineThreads];
+                    const double  iu = pade_u(sm, sp, r0 + u, rows);
+                    const double2 z = wsm[u * NT];
                     wv = make_double2((z.x - wv.x) * iu, (z.y - wv.y) * iu);
                     v[u] = make_double2(fma(-7.2, wv.x, v[u].x), fma(-7.2, wv.y, v[u].y));
                 }
@@ -420,58 +478,79 @@ __global__ void __launch_bounds__(kLineThreads, 1)
     }
 }
 
-// segments per line: a power of two >= kMinSegments (so at most 32 lines share a warp)
-static int solve_geometry(int rows, int *CW, int *P) {
-    int p = kMinSegments;
+// Thread-count variants of the interleaved solve: NT threads per CTA, MINB CTAs per SM.
+struct SolveVariant {
+    int nt, minb;
+};
+static const SolveVariant kVariants[] = {{512, 1}, {256, 2}};
+constexpr int kNumVariants = 2;
+
+// segments per line: a power of two >= NT/32 (so at most 32 lines share a warp)
+static int solve_geometry(int rows, int nt, int *CW, int *P) {
+    int p = nt / 32;
     while (p * kSeg < rows) p <<= 1;
-    if (p > kLineThreads) {
-        set_error("line length %d exceeds %d", rows, kLineThreads * kSeg);
+    if (p > nt) {
+        set_error("line length %d exceeds %d", rows, nt * kSeg);
         return HH_ERR_UNSUPPORTED;
     }
     *P = p;
-    *CW = kLineThreads / p;
+    *CW = nt / p;
     return HH_OK;
 }
 
 int padded_rows(int rows) {
-    int CW, P;
-    if (solve_geometry(rows, &CW, &P) != HH_OK) return rows;
-    return P * kSeg;
+    int best = rows;
+    for (int v = 0; v < kNumVariants; v++) {
+        int CW, P;
+        if (solve_geometry(rows, kVariants[v].nt, &CW, &P) == HH_OK && P * kSeg > best) best = P * kSeg;
+    }
+    return best;
 }
 
-template <int SRC, bool CR> static int launch_solve_t(Plan *p, const double2 *in, double2 *out, int batch) {
+int solve_variant_count() { return kNumVariants; }
+
+template <int SRC, bool CR, int NT, int MINB>
+static int launch_solve_t(Plan *p, const double2 *in, double2 *out, int batch) {
     int CW, P;
-    HH_TRY(solve_geometry(p->rows, &CW, &P));
+    HH_TRY(solve_geometry(p->rows, NT, &CW, &P));
     SrcParams sp;
     sp.dim = p->dim;
     sp.h2 = p->h * p->h;
     sp.k2h2_20 = make_double2(p->k2.x * sp.h2 / 20.0, p->k2.y * sp.h2 / 20.0);
     sp.pl = p->pade_l;
     sp.pu = p->pade_u;
-    const int shm = (int)(sizeof(double2) * kSeg * kLineThreads) * (SRC == 6 ? 2 : 1);
-    HH_CUDA(cudaFuncSetAttribute(k_line_solve<SRC, CR>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
+    sp.linf = p->pade_linf;
+    sp.uinf = p->pade_uinf;
+    const int shm = (int)(sizeof(double2) * kSeg * NT) * (SRC == 6 ? 2 : 1);
+    HH_CUDA(cudaFuncSetAttribute(k_line_solve<SRC, CR, NT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
     // right-hand sides per CTA: enough CTAs to fill the SMs twice, factors reused within a chunk
     const long groups = (p->lines + CW - 1) / CW;
     int rb = 1;
-    while (rb < batch && groups * ((batch + 2 * rb - 1) / (2 * rb)) >= 2L * 148) rb *= 2;
+    while (rb < batch && groups * ((batch + 2 * rb - 1) / (2 * rb)) >= 2L * MINB * 148) rb *= 2;
     const int chunks = (batch + rb - 1) / rb;
     dim3 grid((unsigned)groups, (unsigned)chunks);
-    k_line_solve<SRC, CR><<<grid, kLineThreads, shm, p->ctx->stream>>>(in, out, p->lines, p->rows, p->prow,
-                                                                         p->row_stride, p->field, batch, rb, CW, p->Pv,
-                                                                         p->subt, p->diagt, p->rowc, p->mu, sp);
+    k_line_solve<SRC, CR, NT, MINB><<<grid, NT, shm, p->ctx->stream>>>(in, out, p->lines, p->rows, p->prow,
+                                                                       p->row_stride, p->field, batch, rb, CW, p->Pv,
+                                                                       p->subt, p->diagt, p->rowc, p->mu, sp);
     HH_CUDA(cudaGetLastError());
     p->ctx->launches++;
     return HH_OK;
 }
 
-template <bool CR> static int launch_solve_cr(Plan *p, const double2 *in, double2 *out, int batch, int src) {
+template <bool CR, int NT, int MINB>
+static int launch_solve_v(Plan *p, const double2 *in, double2 *out, int batch, int src) {
     switch (src) {
-    case 0: return launch_solve_t<0, CR>(p, in, out, batch);
-    case 2: return launch_solve_t<2, CR>(p, in, out, batch);
-    case 4: return launch_solve_t<4, CR>(p, in, out, batch);
-    case 6: return launch_solve_t<6, CR>(p, in, out, batch);
+    case 0: return launch_solve_t<0, CR, NT, MINB>(p, in, out, batch);
+    case 2: return launch_solve_t<2, CR, NT, MINB>(p, in, out, batch);
+    case 4: return launch_solve_t<4, CR, NT, MINB>(p, in, out, batch);
+    case 6: return launch_solve_t<6, CR, NT, MINB>(p, in, out, batch);
     default: set_error("source operator order %d", src); return HH_ERR_INVALID;
     }
+}
+
+template <bool CR> static int launch_solve_cr(Plan *p, const double2 *in, double2 *out, int batch, int src) {
+    if (p->variant == 1) return launch_solve_v<CR, 256, 2>(p, in, out, batch, src);
+    return launch_solve_v<CR, 512, 1>(p, in, out, batch, src);
 }
 
 int launch_line_solve(Plan *p, const double2 *in, double2 *out, int batch, int src_order) {

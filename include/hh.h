@@ -106,6 +106,13 @@ int hh_plan3d_create_helmholtz(hh_ctx *ctx, int n, int order, double k_re, doubl
 int hh_plan_destroy(hh_plan *plan);
 long hh_plan_field_size(const hh_plan *plan);  /* complex values per right-hand side */
 
+/* The line solve has several thread mappings (variant 0: 512 threads per block, one block per SM;
+ * 1: 256 threads, two blocks per SM).  hh_plan_tune times each on `batch` right-hand sides and
+ * keeps the fastest (blocking; not during stream capture); set/get select one directly. */
+int hh_plan_tune(hh_plan *plan, int batch);
+int hh_plan_set_variant(hh_plan *plan, int variant);
+int hh_plan_variant(const hh_plan *plan);
+
 /* Solve A u = rhs for `batch` assembled right-hand sides (the reference's solver(System),
  * 2D_Program/solver_functions/solver.c:14, 3D_Program/solver_functions/solver.c:390). */
 int hh_solve(hh_plan *plan, const double *rhs_dev, double *sol_dev, int batch);

@@ -66,6 +66,27 @@ def test_batch_equals_single(ctx, oracle):
         assert np.array_equal(plan.solve_source_host(fs[b]), ub[b])  # bitwise: alone == in batch
 
 
+@pytest.mark.parametrize("n,order,k", [(31, 6, 10.0), (255, 4, 50.0), (1023, 6, 50.0), (2047, 6, 100.0)])
+def test_every_line_solve_variant_matches_oracle(ctx, oracle, n, order, k):
+    """Each thread mapping of the line solve on its own, then hh_plan_tune's choice."""
+    f = _source(n, 7 * n + order)
+    ref = oracle.pipeline_2d(n, order, k, f)
+    plan = hh.Plan.helmholtz(ctx, 2, n, order, k)
+    outs = []
+    for v in range(2):
+        plan.variant = v
+        assert plan.variant == v
+        outs.append(plan.solve_source_host(f[1:-1, 1:-1]))
+        assert_parity_2d(oracle, outs[-1], ref, TOL)
+    assert rel_err(outs[1], outs[0]) < TOL  # same scheme, scans grouped differently: rounding only
+    v = plan.tune(4)
+    assert v in (0, 1)
+    assert np.array_equal(plan.solve_source_host(f[1:-1, 1:-1]), outs[v])
+    with pytest.raises(hh.HHError):
+        plan.variant = 2
+    plan.close()
+
+
 @pytest.mark.parametrize("n,order,k", [(15, 6, 30.0), (31, 6, 30.0), (31, 4, 10.0), (63, 2, 20.0), (127, 6, 30.0)])
 def test_solver3d_fused_source_matches_oracle(ctx, oracle, n, order, k):
     m = W.sine_modes(n + order, 16, min(n, 64), dim=3)
