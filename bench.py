@@ -112,55 +112,74 @@ class _quiet_stdout:
         os.close(self.null)
 
 
-def cpu_baseline(max_seconds: float = 25.0) -> dict:
-    """The reference's own 2D C path (oracle/_ref, OpenMP, all host cores) on a bounded sample:
-    coefficients() + rhs() + LU() + solver() per right-hand side, as its main() runs them."""
+def _reference_runner():
+    """(solve(f), kind, cores): the reference's own 2D C path (oracle/_ref, OpenMP over all host
+    cores) running coefficients() + rhs() + LU() + solver() on one right-hand side, as its main()
+    does; the oracle restatement (one core) where oracle/_ref was not built."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    from hackathon_b200 import workload as W
+    order, k = COMBOS[1]
     try:
         from oracle import Reference2D
         ref = Reference2D()
-        kind = "reference"
-    except Exception:
-        ref = None
-        kind = "port"
-    from oracle import Oracle
-    order, k = COMBOS[1]
-    done, t0 = 0, time.perf_counter()
-    while True:
-        seed = 1000 + done
-        f = W.source_2d(N, W.sine_modes(seed, N_MODES, PMAX), noise_seed=seed + 0x1000000, noise_var=NOISE)
-        if ref is not None:
+
+        def solve(f):
             with _quiet_stdout():
                 ref.pipeline(N, order, k, f, threads=cores)
-        else:
-            Oracle().pipeline_2d(N, order, k, f)
+        return solve, "reference", cores
+    except Exception:
+        from oracle import Oracle
+        orc = Oracle()
+        return (lambda f: orc.pipeline_2d(N, order, k, f)), "port", 1
+
+
+def _baseline_source(i: int):
+    from hackathon_b200 import workload as W
+    seed = 1000 + i
+    return W.source_2d(N, W.sine_modes(seed, N_MODES, PMAX), noise_seed=seed + 0x1000000, noise_var=NOISE,
+                       fast=True)
+
+
+def _sample_text(done: int, kind: str) -> str:
+    order, k = COMBOS[1]
+    return (f"{done} RHS of 2D N=1023 order {order} k={k:g}: coefficients+rhs+LU+solver per RHS "
+            f"({'reference C + project FFT shim; FFTW unavailable on this box' if kind == 'reference' else 'oracle port'})")
+
+
+def cpu_baseline(max_seconds: float = 25.0, max_rhs: int = 8) -> dict:
+    """Bounded sample of the reference CPU path on this host (source generation not timed)."""
+    solve, kind, cores = _reference_runner()
+    done, el = 0, 0.0
+    while done < max_rhs and el < max_seconds:
+        f = _baseline_source(done)
+        t0 = time.perf_counter()
+        solve(f)
+        el += time.perf_counter() - t0
         done += 1
-        el = time.perf_counter() - t0
-        if el > max_seconds or done >= 8:
-            break
-    return {"value": done / el, "unit": "solves/s", "cores": cores if kind == "reference" else 1, "kind": kind,
-            "sample": f"{done} RHS of 2D N=1023 order {order} k={k:g}: coefficients+rhs+LU+solver "
-                      f"(reference C + project FFT shim; FFTW unavailable on this box)"}
+    return {"value": done / el, "unit": "solves/s", "cores": cores, "kind": kind, "sample": _sample_text(done, kind)}
 
 
 def run_reference(args, rank: int) -> None:
+    """The reference arm: each step is one right-hand side through the reference's CPU path."""
     if rank != 0:
         return
-    per_step = []
-    for _ in range(args.warmup + args.steps):
-        b = cpu_baseline(max_seconds=max(5.0, 60.0 / max(1, args.steps + args.warmup)))
-        per_step.append(b)
-    vals = [b["value"] for b in per_step[args.warmup:]] or [per_step[-1]["value"]]
-    v = statistics.median(vals)
+    solve, kind, cores = _reference_runner()
+    srcs = [_baseline_source(i) for i in range(2)]
+    times = []
+    for s in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        solve(srcs[s % 2])
+        times.append(time.perf_counter() - t0)
+    timed = times[args.warmup:] or times[-1:]
+    v = len(timed) / sum(timed)
     line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sine modes + noise)",
-            "config": {"workload": WORKLOAD, "n": N, "batch": 1, "order": COMBOS[1][0], "k": COMBOS[1][1]},
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sine modes + CN(0,1e-3) noise)",
+            "config": {"workload": WORKLOAD, "n": N, "batch_per_step": 1, "order": COMBOS[1][0], "k": COMBOS[1][1]},
             "impl": "reference",
-            "cpu_baseline": {**per_step[-1], "value": v},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": kind,
+                             "sample": _sample_text(len(timed), kind)},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

@@ -1,6 +1,6 @@
 /*
  * libhh3d.so -- the reference 3D program's solver entry points on the GPU
- * (3D_Program/solver_functions/solver.c:390, DST.c:148).  See include/hh_dropin3d.h.
+ * (3D_Program/solver_functions/solver.c:263, DST.c:148).  See include/hh_dropin3d.h.
  */
 #include <complex.h>
 

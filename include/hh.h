@@ -3,7 +3,7 @@
  *
  * The solver follows gonzrona/hackathon: orthonormal DST-I in the constant-coefficient
  * direction(s), shifted tridiagonal line solves in the remaining direction, inverse DST-I
- * (2D_Program/solver_functions/solver.c:14-117, 3D_Program/solver_functions/solver.c:390-540).
+ * (2D_Program/solver_functions/solver.c:14-117, 3D_Program/solver_functions/solver.c:263-413).
  *
  * Conventions
  *  - Complex values are C99 `double _Complex` / interleaved (re, im) doubles; a `const double *`
@@ -114,7 +114,7 @@ int hh_plan_set_variant(hh_plan *plan, int variant);
 int hh_plan_variant(const hh_plan *plan);
 
 /* Solve A u = rhs for `batch` assembled right-hand sides (the reference's solver(System),
- * 2D_Program/solver_functions/solver.c:14, 3D_Program/solver_functions/solver.c:390). */
+ * 2D_Program/solver_functions/solver.c:14, 3D_Program/solver_functions/solver.c:263). */
 int hh_solve(hh_plan *plan, const double *rhs_dev, double *sol_dev, int batch);
 /* Same with host buffers: host-to-device copy, solve, device-to-host copy on the plan's stream. */
 int hh_solve_host(hh_plan *plan, const double *rhs_host, double *sol_host, int batch);

@@ -6,7 +6,7 @@
  *   void forwardDST(...)           -- 2D_Program/solver_functions/DST.c:6
  *   void reverseDST(...)           -- 2D_Program/solver_functions/DST.c:26
  * A reference build links them instead of solver.o and DST.o; its own main(), setup,
- * coefficients(), rhs(), LU() and residual() stay unchanged (see INTEGRATION.md).
+ * coefficients(), rhs(), LU() and residual() stay unchanged.
  *
  * The struct types below reproduce 2D_Program/headers/structs.h:12-30 field for field (same
  * sizes and offsets, 192-byte System) under hh2d_ names so this header can be included next

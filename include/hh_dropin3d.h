@@ -2,7 +2,7 @@
  * hh_dropin3d.h -- drop-in replacement for the 3D program's solver entry points.
  *
  * libhh3d.so exports, with the reference's names and by-value struct ABI:
- *   void solver(System sys)   -- 3D_Program/solver_functions/solver.c:390 (CPU) / :182 (GPU)
+ *   void solver(System sys)   -- 3D_Program/solver_functions/solver.c:263 (CPU) / :55 (GPU)
  *   void DST(int Nx, int Ny, double *b_2D, double *bhat, p1, in1, out1, p2, in2, out2)
  *                             -- 3D_Program/solver_functions/DST.c:148 (FFTW) / :88 (cuFFT)
  *
