@@ -8,6 +8,9 @@
 // buffer, so the solve needs no scratch beyond the output itself.
 #include "hh_internal.cuh"
 
+#include <algorithm>
+#include <cmath>
+
 #include <math.h>
 #include <stdarg.h>
 #include <stdlib.h>
@@ -318,6 +321,25 @@ static int plan_factor(hh_plan *pl, const std::vector<double2> &sub, const std::
         return true;
     };
     p.const_rows = constant(sub) && constant(dia) && constant(sup);
+    // symmetric constant lines (sub == super): the specialised solve; for order 6 it also needs
+    // |10 s - d| well away from zero on every line (partial fractions of A^-1 T^-1)
+    p.sym = p.const_rows;
+    for (int k = 0; k < 4 && p.sym; k++) {
+        const double2 a = sub[(size_t)k * p.rows], b = sup[(size_t)k * p.rows];
+        p.sym = a.x == b.x && a.y == b.y;
+    }
+    p.pf_ok = p.sym;
+    for (int q = 0; q < p.lines && p.pf_ok; q++) {
+        auto line_value = [&](const std::vector<double2> &tb) {
+            const double m0 = mu[q], m1 = mu[(size_t)p.lines + q], m2 = mu[2 * (size_t)p.lines + q];
+            const double2 a = tb[0], b = tb[(size_t)p.rows], c = tb[2 * (size_t)p.rows], d = tb[3 * (size_t)p.rows];
+            return make_double2(((a.x * m0 + b.x * m1) + c.x * m2) + d.x, ((a.y * m0 + b.y * m1) + c.y * m2) + d.y);
+        };
+        const double2 s = line_value(sub), d = line_value(dia);
+        const double  num = std::hypot(10.0 * s.x - d.x, 10.0 * s.y - d.y);
+        p.pf_ok = num >= 0.25 * std::max(std::hypot(s.x, s.y), std::hypot(d.x, d.y));
+    }
+    if (p.sym) p.variant = 2;
     // tables are [4][prow], zero past the last row (neutral rows in the solve)
     auto padded = [&](const std::vector<double2> &t) {
         std::vector<double2> o(4 * (size_t)p.prow, make_double2(0.0, 0.0));

@@ -98,7 +98,9 @@ struct Plan {
     // reciprocal Thomas pivot of the row before each 16-row segment, [segment][line]
     double2 *Pv = nullptr;
     bool     const_rows = false; // stencil row tables constant along the line
-    int      variant = 0;        // line-solve thread mapping (see solve_variant_count / autotune)
+    int      variant = 0;        // line-solve kernel: 0/1 general (512x1, 256x2), 2/3 symmetric (2 or 1 CTA/SM)
+    bool     sym = false;        // const_rows and sub == super on every line (constant k)
+    bool     pf_ok = false;      // order-6 partial fractions well conditioned on every line
     double2 *subt = nullptr, *diagt = nullptr; // sub/diagonal row tables (4 * rows each)
     // super-diagonal(row, line) = rowc[0][row] mu[0][line] + rowc[1][row] mu[1][line] + rowc[2][row] mu[2][line] + rowc[3][row]
     double2 *rowc = nullptr;        // 4 * rows complex

@@ -483,7 +483,7 @@ struct SolveVariant {
     int nt, minb;
 };
 static const SolveVariant kVariants[] = {{512, 1}, {256, 2}};
-constexpr int kNumVariants = 2;
+constexpr int kNumVariants = 2; // plus variants 2, 3: k_line_solve_sym where the plan allows it
 
 // segments per line: a power of two >= NT/32 (so at most 32 lines share a warp)
 static int solve_geometry(int rows, int nt, int *CW, int *P) {
@@ -507,7 +507,7 @@ int padded_rows(int rows) {
     return best;
 }
 
-int solve_variant_count() { return kNumVariants; }
+int solve_variant_count() { return kNumVariants + 2; }
 
 template <int SRC, bool CR, int NT, int MINB>
 static int launch_solve_t(Plan *p, const double2 *in, double2 *out, int batch) {
@@ -553,7 +553,11 @@ template <bool CR> static int launch_solve_cr(Plan *p, const double2 *in, double
     return launch_solve_v<CR, 512, 1>(p, in, out, batch, src);
 }
 
+int launch_line_solve_sym(Plan *p, const double2 *in, double2 *out, int batch, int src_order);
+bool sym_solve_supported(const Plan *p, int src_order);
+
 int launch_line_solve(Plan *p, const double2 *in, double2 *out, int batch, int src_order) {
+    if (p->variant >= 2 && sym_solve_supported(p, src_order)) return launch_line_solve_sym(p, in, out, batch, src_order);
     if (src_order == 6 && !p->pade_l) {
         set_error("order-6 source operator needs a Helmholtz plan");
         return HH_ERR_INVALID;
@@ -563,5 +567,468 @@ int launch_line_solve(Plan *p, const double2 *in, double2 *out, int batch, int s
 }
 
 int segment_count(int rows) { return (rows + kSeg - 1) / kSeg; }
+
+
+// =====================================================================================
+// Symmetric constant-row lines (the Helmholtz plans): k_line_solve_sym
+//
+// For constant k the line matrix is A = d I + s S with S = tridiag(1, 0, 1), the same s below
+// and above the diagonal, and one (d, s) per line.  The kernel specialises the solve above for
+// that case:
+//  * CW (lines per CTA) is a compile-time constant, so every shuffle offset and loop unrolls;
+//  * the segment multipliers of the affine maps depend on the factors only, so their scan
+//    coefficients are formed once per chunk of right-hand sides (tables in shared memory) and
+//    each right-hand side scans only its B values;
+//  * every thread loads the two neighbouring rows of its segment with its own rows, so the
+//    second differences of the compact operator need no exchange;
+//  * order 6: A and the Pade matrix T = 10 I + S are both polynomials in S, so they commute and
+//        A^-1 T^-1 = (s A^-1 - T^-1) / (10 s - d)
+//    The order-6 right-hand side  F = h^2 [a6 g + b6 D2 g - 7.2 T^-1 g]  then gives
+//        u = A^-1 F = A^-1 G + cT T^-1 g,   G = h^2 [(a6 - 7.2 s/(10s - d)) g + b6 D2 g],
+//        cT = 7.2 h^2 / (10 s - d)
+//    two independent solves that run side by side and share every scan and barrier.  The plan
+//    checks |10 s - d| against |d|, |s| on every line before it selects this path.
+// =====================================================================================
+
+// a + b c and a - b c with two fused multiply-adds per component
+__device__ __forceinline__ double2 zfma(double2 a, double2 b, double2 c) {
+    return make_double2(fma(b.x, c.x, fma(-b.y, c.y, a.x)), fma(b.x, c.y, fma(b.y, c.x, a.y)));
+}
+__device__ __forceinline__ double2 zfms(double2 a, double2 b, double2 c) {
+    return make_double2(fma(-b.x, c.x, fma(b.y, c.y, a.x)), fma(-b.x, c.y, fma(-b.y, c.x, a.y)));
+}
+__device__ __forceinline__ double2 zaxpy(double2 a, double b, double2 c) { // a + b c, b real
+    return make_double2(fma(b, c.x, a.x), fma(b, c.y, a.y));
+}
+
+template <int NT> __host__ __device__ constexpr int ilog2_t() { return NT <= 1 ? 0 : 1 + ilog2_t<NT / 2>(); }
+
+template <int NW, int CW> struct SymSmem {
+    double2 AwF[NW][CW], AwB[NW][CW]; // warp totals of the segment multipliers (main solve)
+    double2 BwF[NW][CW], BwB[NW][CW]; // warp totals of the B values, per right-hand side
+    double2 EF[NW][CW], EB[NW][CW];   // value entering each warp
+    double  awF[NW][CW], awB[NW][CW]; // the same for the Pade solve (real multipliers)
+    double2 bwF[NW][CW], bwB[NW][CW];
+    double2 eF[NW][CW], eB[NW][CW];
+    double  pl[9], pu[9];
+};
+
+// Shared-memory reads of the scan tables that the compiler must not hoist out of the loop over
+// right-hand sides (hoisting them would hold every stage multiplier in registers).
+__device__ __forceinline__ double2 lds_keep(const double2 *p) {
+    double2 v;
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];"
+                 : "=d"(v.x), "=d"(v.y)
+                 : "r"(static_cast<uint32_t>(__cvta_generic_to_shared(p))));
+    return v;
+}
+__device__ __forceinline__ double lds_keep(const double *p) {
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(static_cast<uint32_t>(__cvta_generic_to_shared(p))));
+    return v;
+}
+
+// Intra-warp inclusive scan of B over the segments of each line in the warp, with the stage
+// multipliers tab[j * NT] (the thread's own map product at stage j).  FWD composes left to right.
+template <int CW, bool FWD>
+__device__ __forceinline__ double2 sym_warp_scan(double2 B, const double2 *tab, int NT_, int sl) {
+    constexpr int SPW = 32 / CW;
+#pragma unroll
+    for (int j = 0; (1 << j) < SPW; j++) {
+        const double2 Bo = FWD ? shfl_up2(B, CW << j) : shfl_down2(B, CW << j);
+        const double2 m = lds_keep(tab + j * NT_);
+        if (FWD ? (sl >= (1 << j)) : (sl + (1 << j) < SPW)) B = zfma(B, m, Bo);
+    }
+    return B;
+}
+template <int CW, bool FWD>
+__device__ __forceinline__ double2 sym_warp_scan(double2 B, const double *tab, int NT_, int sl) {
+    constexpr int SPW = 32 / CW;
+#pragma unroll
+    for (int j = 0; (1 << j) < SPW; j++) {
+        const double2 Bo = FWD ? shfl_up2(B, CW << j) : shfl_down2(B, CW << j);
+        const double  m = lds_keep(tab + j * NT_);
+        if (FWD ? (sl >= (1 << j)) : (sl + (1 << j) < SPW)) B = zaxpy(B, m, Bo);
+    }
+    return B;
+}
+
+struct SymParams {
+    double  h2;        // h^2
+    double2 k2h2_20;   // k^2 h^2 / 20
+    int     dim;
+    double  linf, uinf;
+    const double *pl, *pu; // Pade factors (rows >= 9 equal linf, uinf)
+};
+
+// One chunk of right-hand sides for the thread's segment: TINT = the warp's rows all lie in
+// [9, rows) (constant Pade factors).
+template <int SRC, int NT, int CW, bool TINT>
+__device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double2 *__restrict__ out, int rows,
+                                          long row_stride, long field, int b_begin, int b_end, long off0,
+                                          bool live, int r0, int sl, int w, int c, const double2 (&Lr)[kSeg],
+                                          const double2 (&ui)[kSeg], double2 ui_in, double2 s, double2 c1, double c2,
+                                          double2 cT, SymSmem<NT / 32, CW> &sm, double2 *pre, const double2 *tabF,
+                                          const double2 *tabB, const double *ttF, const double *ttB,
+                                          const SymParams &sp) {
+    constexpr int NW = NT / 32, SPW = 32 / CW, LOG = ilog2_t<SPW>();
+    constexpr int HALO = (SRC == 4 || SRC == 6) ? 1 : 0;
+    const int     t = threadIdx.x;
+    const double2 zero = make_double2(0.0, 0.0);
+    // forward multiplier of row r0 + k: kept in registers, or (order 6, where registers are
+    // short) re-formed from the reciprocal pivots as the set-up does
+    constexpr bool KEEP_L = SRC != 6;
+    auto LF = [&](int k) -> double2 {
+        if constexpr (KEEP_L) return Lr[k];
+        return cmul(s, k == 0 ? ui_in : ui[k - 1]);
+    };
+    // Pade factors of row r0 + k: the constants in warps whose rows all lie in [9, rows)
+    auto PL = [&](int k) -> double {
+        if constexpr (TINT) return sp.linf;
+        const int r = r0 + k;
+        return r < 9 ? sm.pl[r] : (r < rows ? sp.linf : 0.0);
+    };
+    auto PU = [&](int k) -> double {
+        if constexpr (TINT) return sp.uinf;
+        const int r = r0 + k;
+        return r < 9 ? sm.pu[r] : (r < rows ? sp.uinf : 0.0);
+    };
+
+    auto prefetch = [&](int b) {
+        const double2 *src = in + (long)b * field + off0;
+#pragma unroll
+        for (int k = -HALO; k < kSeg + HALO; k++) {
+            const bool ok = live && r0 + k >= 0 && r0 + k < rows;
+            cp_async16(&pre[(k + 1) * NT + t], ok ? src + (long)k * row_stride : in, ok ? 16 : 0);
+        }
+        cp_async_commit();
+    };
+    prefetch(b_begin);
+    for (int b = b_begin; b < b_end; b++) {
+        double2 v[kSeg], g[kSeg], gm = zero, gp = zero;
+        cp_async_wait_all();
+#pragma unroll
+        for (int k = 0; k < kSeg; k++) v[k] = pre[(k + 1) * NT + t];
+        if constexpr (HALO) {
+            gm = pre[t];
+            gp = pre[(kSeg + 1) * NT + t];
+        }
+        if (b + 1 < b_end) prefetch(b + 1);
+
+        // ---- compact right-hand side (order 6: the A^-1 part; g keeps the source for T^-1)
+        if constexpr (SRC == 2) {
+#pragma unroll
+            for (int k = 0; k < kSeg; k++) v[k] = cscale(v[k], sp.h2);
+        } else if constexpr (SRC == 4 || SRC == 6) {
+            double2 prev = gm;
+#pragma unroll
+            for (int k = 0; k < kSeg; k++) {
+                const double2 gk = v[k], nx = (k == kSeg - 1) ? gp : v[k + 1];
+                const double2 d2 = make_double2(fma(-2.0, gk.x, prev.x + nx.x), fma(-2.0, gk.y, prev.y + nx.y));
+                prev = gk;
+                if constexpr (SRC == 6) g[k] = gk;
+                v[k] = zfma(make_double2(c2 * d2.x, c2 * d2.y), c1, gk); // c2 D2 g + c1 g
+            }
+        }
+
+        // ---- forward elimination: local sweeps from a zero entering value
+        double2 yh = zero, zh = zero;
+#pragma unroll
+        for (int k = 0; k < kSeg; k++) {
+            yh = zfms(v[k], LF(k), yh);
+            if constexpr (SRC == 6) zh = make_double2(fma(-PL(k), zh.x, g[k].x), fma(-PL(k), zh.y, g[k].y));
+        }
+        double2 Bf = sym_warp_scan<CW, true>(yh, tabF + t, NT, sl);
+        double2 bf = zero;
+        if constexpr (SRC == 6) bf = sym_warp_scan<CW, true>(zh, ttF + t, NT, sl);
+        double2 Bfe = shfl_up2(Bf, CW), bfe = zero;
+        if constexpr (SRC == 6) bfe = shfl_up2(bf, CW);
+        if (sl == 0) { Bfe = zero; bfe = zero; }
+        if (sl == SPW - 1) {
+            sm.BwF[w][c] = Bf;
+            if constexpr (SRC == 6) sm.bwF[w][c] = bf;
+        }
+        __syncthreads();
+        if (t < CW) {
+            double2 E = zero;
+#pragma unroll
+            for (int x = 0; x < NW; x++) {
+                sm.EF[x][t] = E;
+                E = zfma(sm.BwF[x][t], sm.AwF[x][t], E);
+            }
+        } else if (SRC == 6 && t >= 32 && t < 32 + CW) {
+            double2 E = zero;
+#pragma unroll
+            for (int x = 0; x < NW; x++) {
+                sm.eF[x][t - 32] = E;
+                E = zaxpy(sm.bwF[x][t - 32], sm.awF[x][t - 32], E);
+            }
+        }
+        __syncthreads();
+        double2 y = zfma(Bfe, lds_keep(tabF + LOG * NT + t), sm.EF[w][c]);
+        double2 z = zero;
+        if constexpr (SRC == 6) z = zaxpy(bfe, lds_keep(ttF + LOG * NT + t), sm.eF[w][c]);
+#pragma unroll
+        for (int k = 0; k < kSeg; k++) {
+            y = zfms(v[k], LF(k), y);
+            v[k] = y;
+            if constexpr (SRC == 6) {
+                z = make_double2(fma(-PL(k), z.x, g[k].x), fma(-PL(k), z.y, g[k].y));
+                g[k] = z;
+            }
+        }
+
+        // ---- back substitution x_r = ui_r (y_r - s x_{r+1});  Pade: w_r = pu_r (z_r - w_{r+1})
+        double2 xh = zero, wh = zero;
+#pragma unroll
+        for (int k = kSeg - 1; k >= 0; k--) {
+            xh = cmul(ui[k], zfms(v[k], s, xh));
+            if constexpr (SRC == 6) wh = make_double2(PU(k) * (g[k].x - wh.x), PU(k) * (g[k].y - wh.y));
+        }
+        double2 Bb = sym_warp_scan<CW, false>(xh, tabB + t, NT, sl);
+        double2 bb = zero;
+        if constexpr (SRC == 6) bb = sym_warp_scan<CW, false>(wh, ttB + t, NT, sl);
+        double2 Bbe = shfl_down2(Bb, CW), bbe = zero;
+        if constexpr (SRC == 6) bbe = shfl_down2(bb, CW);
+        if (sl == SPW - 1) { Bbe = zero; bbe = zero; }
+        if (sl == 0) {
+            sm.BwB[w][c] = Bb;
+            if constexpr (SRC == 6) sm.bwB[w][c] = bb;
+        }
+        __syncthreads();
+        if (t < CW) {
+            double2 E = zero;
+#pragma unroll
+            for (int x = NW - 1; x >= 0; x--) {
+                sm.EB[x][t] = E;
+                E = zfma(sm.BwB[x][t], sm.AwB[x][t], E);
+            }
+        } else if (SRC == 6 && t >= 32 && t < 32 + CW) {
+            double2 E = zero;
+#pragma unroll
+            for (int x = NW - 1; x >= 0; x--) {
+                sm.eB[x][t - 32] = E;
+                E = zaxpy(sm.bwB[x][t - 32], sm.awB[x][t - 32], E);
+            }
+        }
+        __syncthreads();
+        double2 xx = zfma(Bbe, lds_keep(tabB + LOG * NT + t), sm.EB[w][c]);
+        double2 ww = zero;
+        if constexpr (SRC == 6) ww = zaxpy(bbe, lds_keep(ttB + LOG * NT + t), sm.eB[w][c]);
+#pragma unroll
+        for (int k = kSeg - 1; k >= 0; k--) {
+            xx = cmul(ui[k], zfms(v[k], s, xx));
+            v[k] = xx;
+            if constexpr (SRC == 6) {
+                ww = make_double2(PU(k) * (g[k].x - ww.x), PU(k) * (g[k].y - ww.y));
+                v[k] = zfma(v[k], cT, ww);
+            }
+        }
+
+        double2 *dst = out + (long)b * field + off0;
+#pragma unroll
+        for (int k = 0; k < kSeg; k++)
+            if (live && r0 + k < rows) dst[(long)k * row_stride] = v[k];
+    }
+}
+
+// Stage multipliers of the intra-warp scans for one per-segment multiplier a (complex, or real
+// for the Pade solve): tab[j * NT] = the thread's map product before stage j, tab[LOG * NT] =
+// the exclusive product.  Returns the inclusive product, which at the warp's last (forward) or
+// first (backward) segment is the warp total.
+__device__ __forceinline__ double shfl_up1(double v, int off) { return __shfl_up_sync(0xffffffffu, v, off); }
+__device__ __forceinline__ double shfl_down1(double v, int off) { return __shfl_down_sync(0xffffffffu, v, off); }
+__device__ __forceinline__ double2 shfl_up1(double2 v, int off) { return shfl_up2(v, off); }
+__device__ __forceinline__ double2 shfl_down1(double2 v, int off) { return shfl_down2(v, off); }
+__device__ __forceinline__ double  mul1(double a, double b) { return a * b; }
+__device__ __forceinline__ double2 mul1(double2 a, double2 b) { return cmul(a, b); }
+
+template <int CW, bool FWD, typename M>
+__device__ __forceinline__ M sym_scan_table(M a, M *tab, int NT_, int sl, M one) {
+    constexpr int SPW = 32 / CW;
+    int           j = 0;
+#pragma unroll
+    for (; (1 << j) < SPW; j++) {
+        tab[j * NT_] = a;
+        const M o = FWD ? shfl_up1(a, CW << j) : shfl_down1(a, CW << j);
+        if (FWD ? (sl >= (1 << j)) : (sl + (1 << j) < SPW)) a = mul1(a, o);
+    }
+    M e = FWD ? shfl_up1(a, CW) : shfl_down1(a, CW);
+    if (FWD ? sl == 0 : sl == SPW - 1) e = one;
+    tab[j * NT_] = e;
+    return a;
+}
+
+template <int SRC, int NT, int CW, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+    k_line_solve_sym(const double2 *__restrict__ in, double2 *__restrict__ out, int lines, int rows, long row_stride,
+                     long field, int batch, int rb, const double2 *__restrict__ Pv, const double2 *__restrict__ subt,
+                     const double2 *__restrict__ diagt, int prow, const double *__restrict__ mu, SymParams sp) {
+    constexpr int NW = NT / 32, SPW = 32 / CW, LOG = ilog2_t<SPW>();
+    constexpr int HALO = (SRC == 4 || SRC == 6) ? 1 : 0;
+    __shared__ SymSmem<NW, CW> sm;
+    extern __shared__ double2 dyn[];
+    double2 *pre = dyn;                                 // [kSeg + 2][NT]
+    double2 *tabF = pre + (kSeg + 2) * NT;              // [LOG + 1][NT]
+    double2 *tabB = tabF + (LOG + 1) * NT;              // [LOG + 1][NT]
+    double  *ttF = reinterpret_cast<double *>(tabB + (LOG + 1) * NT); // [LOG + 1][NT] (order 6)
+    double  *ttB = ttF + (LOG + 1) * NT;
+    (void)HALO;
+
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int c = t % CW, seg = t / CW, sl = lane / CW;
+    const int q = blockIdx.x * CW + c;
+    const bool live = q < lines;
+    const int  qq = live ? q : 0;
+    const int  r0 = seg * kSeg;
+    const double m0 = mu[qq], m1 = mu[lines + qq], m2 = mu[2 * lines + qq];
+    const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
+
+    // ---- factors of the thread's rows (the set-up's recurrence, same arithmetic)
+    const double2 s = shifted(subt, prow, 0, m0, m1, m2), d = shifted(diagt, prow, 0, m0, m1, m2);
+    double2 Lr[kSeg], ui[kSeg];
+    double2 Af = one, Ab = one;
+    const double2 ui_in = (live && r0 > 0 && r0 < rows) ? Pv[(long)seg * lines + q] : zero; // 1/P of row r0-1
+    {
+        double2 uprev = ui_in;
+#pragma unroll
+        for (int k = 0; k < kSeg; k++) {
+            const int r = r0 + k;
+            Lr[k] = zero;
+            ui[k] = zero;
+            if (live && r < rows) {
+                if (r == 0) ui[k] = first_pivot(d);
+                else ui[k] = factor_step(s, d, s, uprev, Lr[k]);
+            }
+            uprev = ui[k];
+            Af = cmul(Af, make_double2(-Lr[k].x, -Lr[k].y));
+            const double2 tau = cmul(s, ui[k]);
+            Ab = cmul(Ab, make_double2(-tau.x, -tau.y));
+        }
+    }
+
+    // ---- per-line coefficients of the compact right-hand side
+    double2 c1 = one, cT = zero;
+    double  c2 = 0.0;
+    if constexpr (SRC == 4) {
+        c1 = make_double2(sp.h2 * (sp.dim == 2 ? (10.0 + m1) / 12.0 : (8.0 + m1 + m2) / 12.0), 0.0);
+        c2 = sp.h2 / 12.0;
+    } else if constexpr (SRC == 6) {
+        double2 a6;
+        double  b6;
+        if (sp.dim == 2) {
+            const double muq = 12.0 * (m1 - 2.0) / (10.0 + m1);
+            a6 = make_double2(1.6 + muq / 12.0 + (m1 - 2.0) * muq / 360.0 - sp.k2h2_20.x, -sp.k2h2_20.y);
+            b6 = muq / 90.0 + 1.0 / 30.0;
+        } else {
+            const double mx = 12.0 * (m1 - 2.0) / (10.0 + m1), my = 12.0 * (m2 - 2.0) / (10.0 + m2);
+            a6 = make_double2(1.6 + (mx + my) / 12.0 + ((m1 - 2.0) * mx + (m2 - 2.0) * my) / 360.0 +
+                                  (m2 - 2.0) * mx / 90.0 - sp.k2h2_20.x,
+                              -sp.k2h2_20.y);
+            b6 = (mx + my) / 90.0 + 1.0 / 30.0;
+        }
+        const double2 den = crcp(make_double2(10.0 * s.x - d.x, 10.0 * s.y - d.y)); // 1/(10 s - d)
+        const double2 sr = cmul(s, den);
+        c1 = make_double2(sp.h2 * (a6.x - 7.2 * sr.x), sp.h2 * (a6.y - 7.2 * sr.y));
+        c2 = sp.h2 * b6;
+        cT = make_double2(7.2 * sp.h2 * den.x, 7.2 * sp.h2 * den.y);
+    }
+
+    // ---- scan tables (factor-only, shared by every right-hand side of the chunk)
+    {
+        const double2 totF = sym_scan_table<CW, true>(Af, tabF + t, NT, sl, one);
+        const double2 totB = sym_scan_table<CW, false>(Ab, tabB + t, NT, sl, one);
+        if (sl == SPW - 1) sm.AwF[w][c] = totF;
+        if (sl == 0) sm.AwB[w][c] = totB;
+    }
+    if constexpr (SRC == 6) {
+        if (t < 9) {
+            sm.pl[t] = sp.pl[t];
+            sm.pu[t] = sp.pu[t];
+        }
+        __syncthreads();
+        double af = 1.0, ab = 1.0;
+#pragma unroll
+        for (int k = 0; k < kSeg; k++) {
+            const int r = r0 + k;
+            af *= -(r < 9 ? sm.pl[r] : (r < rows ? sp.linf : 0.0));
+            ab *= -(r < 9 ? sm.pu[r] : (r < rows ? sp.uinf : 0.0));
+        }
+        const double totF = sym_scan_table<CW, true>(af, ttF + t, NT, sl, 1.0);
+        const double totB = sym_scan_table<CW, false>(ab, ttB + t, NT, sl, 1.0);
+        if (sl == SPW - 1) sm.awF[w][c] = totF;
+        if (sl == 0) sm.awB[w][c] = totB;
+    }
+    __syncthreads();
+
+    const int  b_begin = blockIdx.y * rb;
+    const int  b_end = min(batch, b_begin + rb);
+    const long off0 = (long)r0 * row_stride + qq;
+    // warps whose rows all lie in [9, rows) use the constant Pade factors
+    const bool tint = (w * SPW * kSeg >= 9) && ((w + 1) * SPW * kSeg <= rows);
+    if (SRC == 6 && tint)
+        sym_chunk<SRC, NT, CW, true>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0, sl, w, c, Lr,
+                                     ui, ui_in, s, c1, c2, cT, sm, pre, tabF, tabB, ttF, ttB, sp);
+    else
+        sym_chunk<SRC, NT, CW, false>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0, sl, w, c, Lr,
+                                      ui, ui_in, s, c1, c2, cT, sm, pre, tabF, tabB, ttF, ttB, sp);
+}
+
+template <int SRC, int CW, int MINB>
+static int launch_sym_t(Plan *p, const double2 *in, double2 *out, int batch) {
+    constexpr int NT = 256, SPW = 32 / CW, LOG = ilog2_t<SPW>();
+    SymParams sp;
+    sp.h2 = p->h * p->h;
+    sp.k2h2_20 = make_double2(p->k2.x * sp.h2 / 20.0, p->k2.y * sp.h2 / 20.0);
+    sp.dim = p->dim;
+    sp.linf = p->pade_linf;
+    sp.uinf = p->pade_uinf;
+    sp.pl = p->pade_l;
+    sp.pu = p->pade_u;
+    const int shm = (int)(sizeof(double2) * ((kSeg + 2) * NT + 2 * (LOG + 1) * NT) +
+                          (SRC == 6 ? sizeof(double) * 2 * (LOG + 1) * NT : 0));
+    HH_CUDA(cudaFuncSetAttribute(k_line_solve_sym<SRC, NT, CW, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
+    const long groups = (p->lines + CW - 1) / CW;
+    int rb = 1;
+    while (rb < batch && groups * ((batch + 2 * rb - 1) / (2 * rb)) >= 2L * MINB * 148) rb *= 2;
+    const int chunks = (batch + rb - 1) / rb;
+    dim3 grid((unsigned)groups, (unsigned)chunks);
+    k_line_solve_sym<SRC, NT, CW, MINB><<<grid, NT, shm, p->ctx->stream>>>(in, out, p->lines, p->rows, p->row_stride,
+                                                                     p->field, batch, rb, p->Pv, p->subt, p->diagt,
+                                                                     p->prow, p->mu, sp);
+    HH_CUDA(cudaGetLastError());
+    p->ctx->launches++;
+    return HH_OK;
+}
+
+template <int SRC, int MINB> static int launch_sym_src(Plan *p, const double2 *in, double2 *out, int batch) {
+    // segments per line: a power of two P >= rows / kSeg with 8 <= P <= 256 (CW = 256 / P lines per CTA)
+    int P = 8;
+    while (P * kSeg < p->rows) P <<= 1;
+    switch (P) {
+    case 8: return launch_sym_t<SRC, 32, MINB>(p, in, out, batch);
+    case 16: return launch_sym_t<SRC, 16, MINB>(p, in, out, batch);
+    case 32: return launch_sym_t<SRC, 8, MINB>(p, in, out, batch);
+    case 64: return launch_sym_t<SRC, 4, MINB>(p, in, out, batch);
+    case 128: return launch_sym_t<SRC, 2, MINB>(p, in, out, batch);
+    case 256: return launch_sym_t<SRC, 1, MINB>(p, in, out, batch);
+    default: set_error("symmetric line solve: %d rows", p->rows); return HH_ERR_UNSUPPORTED;
+    }
+}
+
+bool sym_solve_supported(const Plan *p, int src_order) {
+    return p->sym && p->rows <= 256 * kSeg && (src_order != 6 || (p->pf_ok && p->pade_l));
+}
+
+int launch_line_solve_sym(Plan *p, const double2 *in, double2 *out, int batch, int src_order) {
+    // variant 3: order 6 with one 256-thread CTA per SM and no register cap (no spills)
+    switch (src_order) {
+    case 0: return launch_sym_src<0, 2>(p, in, out, batch);
+    case 2: return launch_sym_src<2, 2>(p, in, out, batch);
+    case 4: return launch_sym_src<4, 2>(p, in, out, batch);
+    case 6: return p->variant == 3 ? launch_sym_src<6, 1>(p, in, out, batch) : launch_sym_src<6, 2>(p, in, out, batch);
+    default: set_error("source operator order %d", src_order); return HH_ERR_INVALID;
+    }
+}
 
 } // namespace hh

@@ -66,24 +66,41 @@ def test_batch_equals_single(ctx, oracle):
         assert np.array_equal(plan.solve_source_host(fs[b]), ub[b])  # bitwise: alone == in batch
 
 
-@pytest.mark.parametrize("n,order,k", [(31, 6, 10.0), (255, 4, 50.0), (1023, 6, 50.0), (2047, 6, 100.0)])
+@pytest.mark.parametrize("n,order,k", [(15, 6, 10.0), (31, 6, 10.0), (63, 2, 30.0), (255, 4, 50.0), (511, 6, 20.0),
+                                       (1023, 6, 50.0), (1023, 4, 10.0), (2047, 6, 100.0)])
 def test_every_line_solve_variant_matches_oracle(ctx, oracle, n, order, k):
-    """Each thread mapping of the line solve on its own, then hh_plan_tune's choice."""
+    """Each line-solve kernel on its own (0/1: general rows, 512 or 256 threads; 2/3: symmetric
+    constant rows with the order-6 partial fractions, 2 or 1 blocks per SM), then
+    hh_plan_tune's choice."""
     f = _source(n, 7 * n + order)
     ref = oracle.pipeline_2d(n, order, k, f)
     plan = hh.Plan.helmholtz(ctx, 2, n, order, k)
+    assert plan.variant == 2  # constant k: the symmetric kernel by default
     outs = []
-    for v in range(2):
+    for v in range(4):
         plan.variant = v
         assert plan.variant == v
         outs.append(plan.solve_source_host(f[1:-1, 1:-1]))
         assert_parity_2d(oracle, outs[-1], ref, TOL)
-    assert rel_err(outs[1], outs[0]) < TOL  # same scheme, scans grouped differently: rounding only
+    for v in range(1, 4):
+        assert rel_err(outs[v], outs[0]) < TOL  # same system, different rounding only
     v = plan.tune(4)
-    assert v in (0, 1)
+    assert v in range(4)
     assert np.array_equal(plan.solve_source_host(f[1:-1, 1:-1]), outs[v])
     with pytest.raises(hh.HHError):
-        plan.variant = 2
+        plan.variant = 4
+    plan.close()
+
+
+def test_symmetric_kernel_assembled_rhs(ctx, oracle):
+    """Helmholtz plan on an assembled right-hand side (no fused operator) through the symmetric
+    kernel, against the reference pipeline."""
+    n, order, k = 1023, 6, 50.0
+    f = _source(n, 17)
+    ref = oracle.pipeline_2d(n, order, k, f)
+    plan = hh.Plan.helmholtz(ctx, 2, n, order, k)
+    sol = plan.solve_host(ref["rhs"])
+    assert_parity_2d(oracle, sol, ref, TOL)
     plan.close()
 
 
