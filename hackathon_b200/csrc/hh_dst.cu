@@ -29,6 +29,8 @@
 
 #include <math.h>
 
+#include <algorithm>
+
 namespace hh {
 
 // ----------------------------------------------------------- in-register DFT ------
@@ -352,6 +354,259 @@ __global__ void __launch_bounds__(DstGeom<M>::NT)
     }
 }
 
+// ------------------------------------------ one warp per line: M = 1024 rows ------
+// The same transform for contiguous rows of length N = 1023 with one warp per line and M = 32 x 32:
+//   lane b loads x_j and the mirror x_{M-j} for j = b + 32 q straight from global memory
+//   (coalesced), forms y_j in registers, runs a 32-point DFT over q, twiddles, and exchanges
+//   through one padded transpose; the second 32-point DFT leaves Y_{b + 32 k2} in lane b.
+//   Post-processing runs on blocks (lane t owns k in [16t, 16t + 16)), so the prefix sum of the
+//   odd outputs is a sequential sum plus one warp scan; the outputs go back through shared
+//   memory so that the global stores are coalesced.
+// Shared-memory traffic per point: transpose (write + read), Y (write + read), S (write + read);
+// the staged design above makes about twice as many passes.
+
+// sin(pi m / 32), m = 0..16
+__device__ __forceinline__ constexpr double sinpi32(int m) {
+    constexpr double s[17] = {0.0,
+                              0.098017140329560601994,
+                              0.19509032201612826785,
+                              0.29028467725446236764,
+                              0.38268343236508977173,
+                              0.47139673682599764856,
+                              0.55557023301960222474,
+                              0.63439328416364549822,
+                              0.7071067811865475244,
+                              0.77301045336273696081,
+                              0.83146961230254523708,
+                              0.88192126434835502971,
+                              0.92387953251128675613,
+                              0.95694033573220886494,
+                              0.98078528040323044913,
+                              0.99518472667219688624,
+                              1.0};
+    return s[m];
+}
+// sin(pi q / 32) and cos(pi q / 32) for q = 0..31
+__device__ __forceinline__ constexpr double sin_q32(int q) { return q <= 16 ? sinpi32(q) : sinpi32(32 - q); }
+__device__ __forceinline__ constexpr double cos_q32(int q) { return q <= 16 ? sinpi32(16 - q) : -sinpi32(q - 16); }
+
+// v * exp(-2 pi i t / 32), t = 0..15: cos(2 pi t/32) = sin(pi (8 - t)/16) = sinpi32(16 - 2t)
+template <int t> __device__ __forceinline__ double2 tw32_mul(double2 v) {
+    if constexpr (t == 0) return v;
+    else if constexpr (t == 8) return make_double2(v.y, -v.x);
+    else if constexpr (t == 4) {
+        constexpr double r = sinpi32(8);
+        return make_double2((v.x + v.y) * r, (v.y - v.x) * r);
+    } else if constexpr (t == 12) {
+        constexpr double r = sinpi32(8);
+        return make_double2((v.y - v.x) * r, -(v.x + v.y) * r);
+    } else {
+        constexpr double c = t < 8 ? sinpi32(16 - 2 * t) : -sinpi32(2 * t - 16), s = sinpi32(t < 8 ? 2 * t : 32 - 2 * t);
+        return make_double2(fma(v.x, c, v.y * s), fma(v.y, c, -(v.x * s)));
+    }
+}
+template <int SPAN, int J> struct Dif32Butterflies {
+    __device__ __forceinline__ static void run(double2 (&v)[32], int start) {
+        if constexpr (J < SPAN) {
+            const double2 a = v[start + J], b = v[start + J + SPAN];
+            v[start + J] = cadd(a, b);
+            v[start + J + SPAN] = tw32_mul<J * (16 / SPAN)>(csub(a, b));
+            Dif32Butterflies<SPAN, J + 1>::run(v, start);
+        }
+    }
+};
+template <int SPAN, int START> struct Dif32Stage {
+    __device__ __forceinline__ static void run(double2 (&v)[32]) {
+        if constexpr (START < 32) {
+            Dif32Butterflies<SPAN, 0>::run(v, START);
+            Dif32Stage<SPAN, START + 2 * SPAN>::run(v);
+        }
+    }
+};
+template <int SPAN> struct Dif32All {
+    __device__ __forceinline__ static void run(double2 (&v)[32]) {
+        if constexpr (SPAN >= 1) {
+            Dif32Stage<SPAN, 0>::run(v);
+            Dif32All<SPAN / 2>::run(v);
+        }
+    }
+};
+// forward 32-point DFT in registers; X[k] = v[bitrev5(k)]
+__device__ __forceinline__ void dft32(double2 (&v)[32]) { Dif32All<16>::run(v); }
+
+constexpr int kDstWarps = 2;                  // warps per CTA
+constexpr int kDstWarpBuf = 1088;             // double2 per buffer: max(32 x 33, 1024 + 1024/16)
+__host__ __device__ constexpr int hibit(int k) { return k <= 1 ? 0 : 1 + hibit(k >> 1); }
+__host__ __device__ constexpr int t33(int i, int j) { return 33 * i + j; }          // transpose layout
+__host__ __device__ constexpr int p16(int k) { return k + (k >> 4); }               // Y layout
+__host__ __device__ constexpr int o33(int p) { return 33 * (p >> 5) + (p & 31); }   // output layout
+
+// bounded wait on an mbarrier phase; false if it did not complete within the budget
+__device__ __forceinline__ bool mbar_wait_parity(uint64_t *bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (long it = 0; it < (1L << 26); it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Persistent warps: warp w of the grid transforms lines w, w + W, w + 2W, ... (W warps in all),
+// each line (plane = g / nlines, line = g % nlines) at in + plane*in_plane + line*in_ld with x_1..x_N
+// at offsets 0..N-1, and likewise for the output.  Each warp owns two line buffers: while it
+// transforms one line, the TMA brings in its next.  in and out may be the same buffer.
+__global__ void __launch_bounds__(32 * kDstWarps, 3)
+    k_dst1_w1024(const double2 *in, double2 *out, long nlines, long nplanes, long in_ld, long out_ld, long in_plane,
+                 long out_plane, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
+    constexpr int      M = 1024, N = M - 1;
+    constexpr uint32_t kBytes = N * 16;
+    extern __shared__ __align__(128) unsigned char dsm[];
+    const int  lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+    uint64_t  *bar = reinterpret_cast<uint64_t *>(dsm) + 2 * wq;
+    double2   *bufs = reinterpret_cast<double2 *>(dsm + 16 * kDstWarps) + 2 * wq * kDstWarpBuf;
+    const long total = nlines * nplanes;
+    const long stride = (long)gridDim.x * kDstWarps;
+    const long g0 = (long)blockIdx.x * kDstWarps + wq;
+    if (g0 >= total) return; // whole warp
+    const double2 zero = make_double2(0.0, 0.0);
+
+    auto src_of = [&](long g) { return in + (g / nlines) * in_plane + (g % nlines) * in_ld; };
+    auto dst_of = [&](long g) { return out + (g / nlines) * out_plane + (g % nlines) * out_ld; };
+    if (lane == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    if (lane == 0) {
+        mbar_expect_tx(&bar[0], kBytes);
+        tma_bulk_load(bufs, src_of(g0), kBytes, &bar[0]);
+        if (g0 + stride < total) {
+            mbar_expect_tx(&bar[1], kBytes);
+            tma_bulk_load(bufs + kDstWarpBuf, src_of(g0 + stride), kBytes, &bar[1]);
+        }
+    }
+
+    // per-lane constants: sin, cos(pi lane / M) and the twiddles W_M^{lane a}, W_M^{8 lane b}
+    const double sb = __ldg(sn + lane), cb = __ldg(sn + M / 2 - lane);
+    double2      twa[8], twb[4];
+#pragma unroll
+    for (int a = 0; a < 8; a++) twa[a] = __ldg(tw + ((lane * a) & (M - 1)));
+#pragma unroll
+    for (int b = 0; b < 4; b++) twb[b] = __ldg(tw + ((8 * lane * b) & (M - 1)));
+    const double coef = sqrt(2.0 / M);
+
+    int  i = 0;
+    long failed = -1;
+    for (long g = g0; g < total; g += stride, i++) {
+        double2 *buf = bufs + (i & 1) * kDstWarpBuf;
+        if (!mbar_wait_parity(&bar[i & 1], (i >> 1) & 1)) {
+            if (lane == 0) atomicExch(err, 1);
+            failed = g;
+            break;
+        }
+
+        // The per-lane sines and twiddles are re-formed for every line: an empty asm hides their
+        // inputs from loop-invariant hoisting, which would otherwise pin ~90 registers.
+        double sbl = sb, cbl = cb;
+        asm volatile("" : "+d"(sbl), "+d"(cbl));
+#pragma unroll
+        for (int a = 0; a < 8; a++) asm volatile("" : "+d"(twa[a].x), "+d"(twa[a].y));
+#pragma unroll
+        for (int b = 0; b < 4; b++) asm volatile("" : "+d"(twb[b].x), "+d"(twb[b].y));
+
+        // ---- y_j = sin(pi j/M)(x_j + x_{M-j}) + (x_j - x_{M-j})/2,  j = lane + 32 q
+        double2 v[32];
+#pragma unroll
+        for (int q = 0; q < 32; q++) {
+            const int j = lane + 32 * q;
+            double2   a = zero, m = zero;
+            if (q > 0 || lane > 0) {
+                a = buf[j - 1];
+                m = buf[M - j - 1];
+            }
+            const double s = fma(sbl, cos_q32(q), cbl * sin_q32(q)); // sin(pi (lane + 32 q) / M)
+            v[q] = make_double2(fma(s, a.x + m.x, 0.5 * (a.x - m.x)), fma(s, a.y + m.y, 0.5 * (a.y - m.y)));
+        }
+        __syncwarp(); // the raw line is consumed; the buffer becomes the exchange area
+
+        // ---- 32-point DFTs over q, twiddle W_M^{lane k1}, transpose
+        dft32(v);
+#pragma unroll
+        for (int k1 = 0; k1 < 32; k1++)
+            buf[t33(k1, lane)] = k1 ? cmul(v[bitrev_c<32>(k1)], cmul(twa[k1 & 7], twb[k1 >> 3])) : v[0];
+        __syncwarp();
+#pragma unroll
+        for (int j1 = 0; j1 < 32; j1++) v[j1] = buf[t33(lane, j1)];
+        __syncwarp();
+
+        // ---- 32-point DFTs over j1: Y_{lane + 32 k2} = v[bitrev(k2)]
+        dft32(v);
+#pragma unroll
+        for (int k2 = 0; k2 < 32; k2++) buf[p16(lane + 32 * k2)] = v[bitrev_c<32>(k2)];
+        __syncwarp();
+
+        // ---- post-processing on blocks k = 16 lane + u
+        double2 cs[16], ev[16];
+        double2 run = zero;
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            const int     k = 16 * lane + u;
+            const double2 yk = buf[p16(k)];
+            if (k == 0) {
+                cs[u] = make_double2(0.5 * yk.x, 0.5 * yk.y);
+                ev[u] = zero;
+            } else {
+                const double2 ym = buf[p16(M - k)];
+                cs[u] = make_double2(0.5 * (yk.x + ym.x), 0.5 * (yk.y + ym.y));
+                ev[u] = make_double2(0.5 * (ym.y - yk.y), -0.5 * (ym.x - yk.x)); // (Y_{M-k} - Y_k)/(2i)
+            }
+            run = cadd(run, cs[u]);
+            cs[u] = run;
+        }
+        double2 incl = run;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const double ox = __shfl_up_sync(0xffffffffu, incl.x, off), oy = __shfl_up_sync(0xffffffffu, incl.y, off);
+            if (lane >= off) { incl.x += ox; incl.y += oy; }
+        }
+        const double2 pre = csub(incl, run);
+        __syncwarp(); // every read of Y is done
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            const int k = 16 * lane + u;
+            buf[o33(2 * k)] = cscale(cadd(pre, cs[u]), coef);     // S_{2k+1} at offset 2k
+            if (k > 0) buf[o33(2 * k - 1)] = cscale(ev[u], coef); // S_{2k}   at offset 2k-1
+        }
+        __syncwarp();
+        double2 *dst = dst_of(g);
+#pragma unroll
+        for (int q = 0; q < 32; q++) {
+            const int p = lane + 32 * q;
+            if (p < N) dst[p] = buf[o33(p)];
+        }
+        __syncwarp();
+        // the buffer is free again: bring in the line after next (generic-proxy reads of the
+        // buffer are ordered before the asynchronous copy that overwrites it)
+        if (lane == 0 && g + 2 * stride < total) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(&bar[i & 1], kBytes);
+            tma_bulk_load(buf, src_of(g + 2 * stride), kBytes, &bar[i & 1]);
+        }
+    }
+    // after an expired wait, give the copies still in flight (this buffer's and the next one's)
+    // a bounded chance to land before the CTA's shared memory is released
+    if (failed >= 0 && lane == 0) {
+        mbar_wait_parity(&bar[i & 1], (i >> 1) & 1);
+        if (failed + stride < total) mbar_wait_parity(&bar[(i + 1) & 1], ((i + 1) >> 1) & 1);
+    }
+}
+
 // ---------------------------------------------- direct DST (any n, dense sine matrix) ----
 // out_k = sqrt(2/(n+1)) sum_m in_m sin(pi (k+1)(m+1)/(n+1)); `mat` holds the n*n sines.
 constexpr int kDenseThreads = 128;
@@ -458,6 +713,24 @@ template <int M, bool IS, bool OS> static int launch_fft(Ctx *c, const DstArgs &
     return HH_OK;
 }
 
+static int launch_w1024(Ctx *c, const DstArgs &a) {
+    const double2 *tw;
+    const double  *sn;
+    HH_TRY(tables_for(c, 1024, &tw, &sn));
+    const int shm = 16 * kDstWarps + (int)(sizeof(double2) * kDstWarpBuf * 2 * kDstWarps);
+    HH_CUDA(cudaFuncSetAttribute(k_dst1_w1024, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
+    int dev = 0, sms = 148;
+    HH_CUDA(cudaGetDevice(&dev));
+    HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long lines = a.nlines * a.planes;
+    const long ctas = std::min<long>((lines + kDstWarps - 1) / kDstWarps, 3L * sms);
+    k_dst1_w1024<<<(unsigned)ctas, 32 * kDstWarps, shm, c->stream>>>(a.in, a.out, a.nlines, a.planes, a.in_ld, a.out_ld,
+                                                                     a.in_plane, a.out_plane, tw, sn, c->err_word);
+    HH_CUDA(cudaGetLastError());
+    c->launches++;
+    return HH_OK;
+}
+
 template <bool IS, bool OS> static int launch_dispatch(Ctx *c, int n, const DstArgs &a) {
     if (n < 1) { set_error("DST length must be >= 1 (got %d)", n); return HH_ERR_INVALID; }
     if (a.nlines <= 0 || a.planes <= 0) return HH_OK;
@@ -466,6 +739,7 @@ template <bool IS, bool OS> static int launch_dispatch(Ctx *c, int n, const DstA
         set_error("DST rows must be 16-byte aligned");
         return HH_ERR_INVALID;
     }
+    if (n == 1023 && !IS && !OS) return launch_w1024(c, a);
     switch (n + 1) {
     case 64: return launch_fft<64, IS, OS>(c, a);
     case 128: return launch_fft<128, IS, OS>(c, a);

@@ -52,6 +52,21 @@ def test_dst_is_an_involution(ctx):
     assert rel_err(_host(t), x) < 1e-13
 
 
+@pytest.mark.parametrize("n", [255, 1023, 2047])
+def test_dst_rows_pitched(ctx, oracle, n):
+    """Rows inside wider pitched buffers (in_ld, out_ld > n), with a line count that leaves the
+    last CTA partly empty."""
+    rows, ld_in, ld_out = 21, n + 9, n + 3
+    rng = np.random.default_rng(7 * n)
+    x = rng.standard_normal((rows, ld_in)) + 1j * rng.standard_normal((rows, ld_in))
+    out = torch.full((rows, ld_out), 7.0 + 7.0j, dtype=torch.complex128, device="cuda")
+    ctx.dst1_rows(n, rows, _dev(x), out, in_ld=ld_in, out_ld=ld_out)
+    ctx.synchronize()
+    o = _host(out)
+    assert rel_err(o[:, :n], oracle.dst1_rows(x[:, :n])) < 1e-13
+    assert np.all(o[:, n:] == 7.0 + 7.0j)  # nothing written past the line
+
+
 @pytest.mark.parametrize("n,ncols,planes", [(255, 255, 3), (63, 100, 2), (100, 37, 2), (1023, 64, 1), (7, 5, 4)])
 def test_dst_cols_matches_oracle(ctx, oracle, n, ncols, planes):
     rng = np.random.default_rng(n + ncols)
