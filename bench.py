@@ -193,6 +193,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--batch", type=int, default=BATCH, help="right-hand sides per step (profiling runs)")
+    ap.add_argument("--variant", type=int, default=None,
+                    help="force one line-solve kernel variant instead of hh_plan_tune (profiling runs)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -220,7 +222,10 @@ def main():
     ctx = hh.Context(local, stream=st.cuda_stream)
     plans = [hh.Plan.helmholtz(ctx, 2, N, o, k) for o, k in COMBOS]
     for p in plans:
-        p.tune(batch)  # pick the line-solve thread mapping (setup, outside the timed region)
+        if args.variant is None:
+            p.tune(batch)  # pick the line-solve kernel (setup, outside the timed region)
+        else:
+            p.variant = args.variant
     f_host = sources(batch, index=1 + rank)
     f = torch.from_numpy(f_host).cuda()
     u = torch.empty_like(f)
@@ -298,7 +303,8 @@ def main():
         pin_in = torch.from_numpy(f_host).pin_memory()
         pin_out = torch.empty_like(pin_in).pin_memory()
         e2e_steps = max(2, min(args.steps, 6))
-        hh.check(hh.lib().hh_solve_source_host(plans[0].h, pin_in.data_ptr(), pin_out.data_ptr(), batch), "e2e")
+        for p in plans:  # warm-up: staging buffer and copy streams exist before the timed region
+            hh.check(hh.lib().hh_solve_source_host(p.h, pin_in.data_ptr(), pin_out.data_ptr(), batch), "e2e")
         barrier()
         t0 = time.perf_counter()
         for s in range(e2e_steps):
@@ -319,7 +325,8 @@ def main():
             "config": {"workload": WORKLOAD, "n": N, "batch_per_gpu": batch, "orders": [4, 6],
                        "k": [10, 50, 200], "form": "plain FP64", "rhs_assembly": "fused",
                        "l2": "inputs 1.07 GB per step > 126 MB L2 (no flush needed)",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}",
+                       "line_solve_variants": [p.variant for p in plans]},
             "gpoints_per_s": value * N * N / 1e9,
             "stage_ms_per_solve_batch": {nm: stage_ms[i] / max(1, timed) for i, nm in enumerate(stage_names)},
             "roofline": {"bound": "hbm", "kernel": stage_names[dom], "achieved": achieved, "peak": peak,

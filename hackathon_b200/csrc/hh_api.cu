@@ -21,12 +21,13 @@
 
 struct hh_ctx {
     hh::Ctx c;
+    // device staging for hh_solve_host / hh_solve_source_host, shared by the context's plans
+    // (host-buffer solves are synchronous, so one call uses it at a time)
+    double2 *stage = nullptr;
+    long     stage_elems = 0;
 };
 struct hh_plan {
     hh::Plan p;
-    // host staging for hh_solve_host / hh_solve_source_host
-    double2 *stage = nullptr;
-    long     stage_elems = 0;
 };
 
 namespace hh {
@@ -109,6 +110,10 @@ extern "C" int hh_ctx_destroy(hh_ctx *x) {
     for (auto &kv : x->c.sn) cudaFree(kv.second);
     for (auto &kv : x->c.dense) cudaFree(kv.second);
     cudaFree(x->c.err_word);
+    cudaFree(x->stage);
+    for (cudaEvent_t e : x->c.chunk_ev) cudaEventDestroy(e);
+    if (x->c.copy_in) cudaStreamDestroy(x->c.copy_in);
+    if (x->c.copy_out) cudaStreamDestroy(x->c.copy_out);
     if (x->c.own_stream) cudaStreamDestroy(x->c.stream);
     delete x;
     return HH_OK;
@@ -265,7 +270,6 @@ static void plan_free(hh_plan *pl) {
     cudaFree(p.mu);
     cudaFree(p.pade_l);
     cudaFree(p.pade_u);
-    cudaFree(pl->stage);
 }
 
 // [1 10 1] Pade factors along the line direction (the reference's constant-coefficient solves,
@@ -622,6 +626,9 @@ extern "C" int hh_solve_source(hh_plan *pl, const double *f, double *u, int batc
     return stage_mark(*p.ctx, 3);
 }
 
+// Host buffers: the batch goes through in chunks so that the host-to-device copy of chunk i+1,
+// the solve of chunk i and the device-to-host copy of chunk i-1 overlap (separate copy streams,
+// ordered by events).  Host memory should be pinned for the copies to run asynchronously.
 static int solve_host_common(hh_plan *pl, const double *in_host, double *out_host, int batch, bool source) {
     HH_TRY(check_batch(pl, batch));
     if (batch == 0) return HH_OK;
@@ -629,20 +636,48 @@ static int solve_host_common(hh_plan *pl, const double *in_host, double *out_hos
     Plan &p = pl->p;
     Ctx  *c = p.ctx;
     HH_CUDA(cudaSetDevice(c->device));
+    hh_ctx    *owner = reinterpret_cast<hh_ctx *>(c); // Ctx is the first member of hh_ctx
     const long need = p.field * batch;
-    if (pl->stage_elems < need) {
-        cudaFree(pl->stage);
-        pl->stage = nullptr;
-        pl->stage_elems = 0;
-        HH_CUDA(cudaMalloc(&pl->stage, sizeof(double2) * (size_t)need));
-        pl->stage_elems = need;
+    if (owner->stage_elems < need) {
+        HH_CUDA(cudaStreamSynchronize(c->stream));
+        cudaFree(owner->stage);
+        owner->stage = nullptr;
+        owner->stage_elems = 0;
+        HH_CUDA(cudaMalloc(&owner->stage, sizeof(double2) * (size_t)need));
+        owner->stage_elems = need;
     }
-    const size_t bytes = sizeof(double2) * (size_t)need;
-    HH_CUDA(cudaMemcpyAsync(pl->stage, in_host, bytes, cudaMemcpyHostToDevice, c->stream));
-    const double *d = (const double *)pl->stage;
-    HH_TRY(source ? hh_solve_source(pl, d, (double *)pl->stage, batch) : hh_solve(pl, d, (double *)pl->stage, batch));
-    HH_CUDA(cudaMemcpyAsync(out_host, pl->stage, bytes, cudaMemcpyDeviceToHost, c->stream));
-    hh_ctx *owner = reinterpret_cast<hh_ctx *>(c); // Ctx is the first member of hh_ctx
+    // chunks of at least 4 MB of field data, at most 8 chunks
+    int nchunk = (int)std::min<long>(8, std::max<long>(1, (long)(sizeof(double2) * need) / (4L << 20)));
+    nchunk = std::min(nchunk, batch);
+    if (!c->copy_in) {
+        HH_CUDA(cudaStreamCreateWithFlags(&c->copy_in, cudaStreamNonBlocking));
+        HH_CUDA(cudaStreamCreateWithFlags(&c->copy_out, cudaStreamNonBlocking));
+    }
+    while ((int)c->chunk_ev.size() < 2 * 8 + 1) {
+        cudaEvent_t e;
+        HH_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c->chunk_ev.push_back(e);
+    }
+    // copies start after the work already queued on the context stream
+    HH_CUDA(cudaEventRecord(c->chunk_ev[16], c->stream));
+    HH_CUDA(cudaStreamWaitEvent(c->copy_in, c->chunk_ev[16], 0));
+    const int per = (batch + nchunk - 1) / nchunk;
+    for (int i = 0, b0 = 0; b0 < batch; i++, b0 += per) {
+        const int    nb = std::min(per, batch - b0);
+        const size_t off = (size_t)p.field * b0, bytes = sizeof(double2) * (size_t)p.field * nb;
+        double2     *d = owner->stage + off;
+        HH_CUDA(cudaMemcpyAsync(d, in_host + 2 * off, bytes, cudaMemcpyHostToDevice, c->copy_in));
+        HH_CUDA(cudaEventRecord(c->chunk_ev[2 * i], c->copy_in));
+        HH_CUDA(cudaStreamWaitEvent(c->stream, c->chunk_ev[2 * i], 0));
+        HH_TRY(source ? hh_solve_source(pl, (const double *)d, (double *)d, nb)
+                      : hh_solve(pl, (const double *)d, (double *)d, nb));
+        HH_CUDA(cudaEventRecord(c->chunk_ev[2 * i + 1], c->stream));
+        HH_CUDA(cudaStreamWaitEvent(c->copy_out, c->chunk_ev[2 * i + 1], 0));
+        HH_CUDA(cudaMemcpyAsync(out_host + 2 * off, d, bytes, cudaMemcpyDeviceToHost, c->copy_out));
+    }
+    // the context stream sees the copies complete before anything queued after this call
+    HH_CUDA(cudaEventRecord(c->chunk_ev[16], c->copy_out));
+    HH_CUDA(cudaStreamWaitEvent(c->stream, c->chunk_ev[16], 0));
     return hh_ctx_synchronize(owner);
 }
 

@@ -78,6 +78,9 @@ struct Ctx {
     std::vector<cudaEvent_t> ev_pending;          // groups of 4 events per timed solve
     double                   stage_ms[3] = {0, 0, 0};
     long long                timed_solves = 0;
+    // host-buffer solves: copy streams and per-chunk events (created on first use)
+    cudaStream_t             copy_in = nullptr, copy_out = nullptr;
+    std::vector<cudaEvent_t> chunk_ev;
 };
 
 int tables_for(Ctx *c, int m, const double2 **tw, const double **sn);

@@ -104,6 +104,22 @@ def test_symmetric_kernel_assembled_rhs(ctx, oracle):
     plan.close()
 
 
+def test_host_path_chunked_equals_device_path(ctx):
+    """Host-buffer solves run in overlapped chunks (copies on their own streams); the result is
+    bitwise the device-buffer solve of the whole batch."""
+    torch = pytest.importorskip("torch")
+    n, B = 1023, 8
+    fs = np.stack([_source(n, 300 + b)[1:-1, 1:-1] for b in range(B)])
+    plan = hh.Plan.helmholtz(ctx, 2, n, 6, 50.0)
+    host = plan.solve_source_host(torch.from_numpy(fs).pin_memory().numpy())
+    f = torch.from_numpy(fs).cuda()
+    u = torch.empty_like(f)
+    plan.solve_source(f, u, B)
+    ctx.synchronize()
+    assert np.array_equal(host, u.cpu().numpy())
+    plan.close()
+
+
 @pytest.mark.parametrize("n,order,k", [(15, 6, 30.0), (31, 6, 30.0), (31, 4, 10.0), (63, 2, 20.0), (127, 6, 30.0)])
 def test_solver3d_fused_source_matches_oracle(ctx, oracle, n, order, k):
     m = W.sine_modes(n + order, 16, min(n, 64), dim=3)
