@@ -51,6 +51,8 @@
 // HBM traffic.
 #include "hh_internal.cuh"
 
+#include <algorithm>
+
 namespace hh {
 
 struct LineCoef {
@@ -483,7 +485,7 @@ struct SolveVariant {
     int nt, minb;
 };
 static const SolveVariant kVariants[] = {{512, 1}, {256, 2}};
-constexpr int kNumVariants = 2; // plus variants 2, 3: k_line_solve_sym where the plan allows it
+constexpr int kNumVariants = 2; // plus variants 2..4: k_line_solve_sym where the plan allows it
 
 // segments per line: a power of two >= NT/32 (so at most 32 lines share a warp)
 static int solve_geometry(int rows, int nt, int *CW, int *P) {
@@ -507,7 +509,7 @@ int padded_rows(int rows) {
     return best;
 }
 
-int solve_variant_count() { return kNumVariants + 2; }
+int solve_variant_count() { return kNumVariants + 3; }
 
 template <int SRC, bool CR, int NT, int MINB>
 static int launch_solve_t(Plan *p, const double2 *in, double2 *out, int batch) {
@@ -603,13 +605,13 @@ __device__ __forceinline__ double2 zaxpy(double2 a, double b, double2 c) { // a 
 
 template <int NT> __host__ __device__ constexpr int ilog2_t() { return NT <= 1 ? 0 : 1 + ilog2_t<NT / 2>(); }
 
-template <int NW, int CW> struct SymSmem {
+template <int NW, int CW, int NR> struct SymSmem {
     double2 AwF[NW][CW], AwB[NW][CW]; // warp totals of the segment multipliers (main solve)
-    double2 BwF[NW][CW], BwB[NW][CW]; // warp totals of the B values, per right-hand side
-    double2 EF[NW][CW], EB[NW][CW];   // value entering each warp
     double  awF[NW][CW], awB[NW][CW]; // the same for the Pade solve (real multipliers)
-    double2 bwF[NW][CW], bwB[NW][CW];
-    double2 eF[NW][CW], eB[NW][CW];
+    double2 BwF[NR][NW][CW], BwB[NR][NW][CW]; // warp totals of the B values, per right-hand side
+    double2 EF[NR][NW][CW], EB[NR][NW][CW];   // value entering each warp
+    double2 bwF[NR][NW][CW], bwB[NR][NW][CW];
+    double2 eF[NR][NW][CW], eB[NR][NW][CW];
     double  pl[9], pu[9];
 };
 
@@ -661,18 +663,22 @@ struct SymParams {
     const double *pl, *pu; // Pade factors (rows >= 9 equal linf, uinf)
 };
 
-// One chunk of right-hand sides for the thread's segment: TINT = the warp's rows all lie in
-// [9, rows) (constant Pade factors).
-template <int SRC, int NT, int CW, bool TINT>
+// One chunk of right-hand sides for the thread's segment, NR of them side by side (independent
+// dependency chains, shared barriers).  TINT = the warp's rows all lie in [9, rows) (constant
+// Pade factors).
+template <int SRC, int NT, int CW, bool TINT, int NR>
 __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double2 *__restrict__ out, int rows,
                                           long row_stride, long field, int b_begin, int b_end, long off0,
                                           bool live, int r0, int sl, int w, int c, const double2 (&Lr)[kSeg],
                                           const double2 (&ui)[kSeg], double2 ui_in, double2 s, double2 c1, double c2,
-                                          double2 cT, SymSmem<NT / 32, CW> &sm, double2 *pre, const double2 *tabF,
-                                          const double2 *tabB, const double *ttF, const double *ttB,
-                                          const SymParams &sp) {
+                                          double2 cT, SymSmem<NT / 32, CW, NR> &sm, double2 *pre,
+                                          const double2 *tabF, const double2 *tabB, const double *ttF,
+                                          const double *ttB, const SymParams &sp) {
     constexpr int NW = NT / 32, SPW = 32 / CW, LOG = ilog2_t<SPW>();
     constexpr int HALO = (SRC == 4 || SRC == 6) ? 1 : 0;
+    constexpr int SLOTS = kSeg + 2;
+    // cross-warp sequential passes: main solve on threads [0, CW NR), Pade solve on [128, 128 + CW NR)
+    static_assert(CW * NR <= 128 && NT >= 256, "cross-warp thread ranges");
     const int     t = threadIdx.x;
     const double2 zero = make_double2(0.0, 0.0);
     // forward multiplier of row r0 + k: kept in registers, or (order 6, where registers are
@@ -695,140 +701,206 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
     };
 
     auto prefetch = [&](int b) {
-        const double2 *src = in + (long)b * field + off0;
 #pragma unroll
-        for (int k = -HALO; k < kSeg + HALO; k++) {
-            const bool ok = live && r0 + k >= 0 && r0 + k < rows;
-            cp_async16(&pre[(k + 1) * NT + t], ok ? src + (long)k * row_stride : in, ok ? 16 : 0);
+        for (int r = 0; r < NR; r++) {
+            const bool     okb = live && b + r < b_end;
+            const double2 *src = in + (long)(okb ? b + r : 0) * field + off0;
+#pragma unroll
+            for (int k = -HALO; k < kSeg + HALO; k++) {
+                const bool ok = okb && r0 + k >= 0 && r0 + k < rows;
+                cp_async16(&pre[(r * SLOTS + k + 1) * NT + t], ok ? src + (long)k * row_stride : in, ok ? 16 : 0);
+            }
         }
         cp_async_commit();
     };
     prefetch(b_begin);
-    for (int b = b_begin; b < b_end; b++) {
-        double2 v[kSeg], g[kSeg], gm = zero, gp = zero;
+    for (int b = b_begin; b < b_end; b += NR) {
+        double2 v[NR][kSeg], g[NR][kSeg], gm[NR], gp[NR];
         cp_async_wait_all();
 #pragma unroll
-        for (int k = 0; k < kSeg; k++) v[k] = pre[(k + 1) * NT + t];
-        if constexpr (HALO) {
-            gm = pre[t];
-            gp = pre[(kSeg + 1) * NT + t];
+        for (int r = 0; r < NR; r++) {
+#pragma unroll
+            for (int k = 0; k < kSeg; k++) v[r][k] = pre[(r * SLOTS + k + 1) * NT + t];
+            gm[r] = zero;
+            gp[r] = zero;
+            if constexpr (HALO) {
+                gm[r] = pre[(r * SLOTS) * NT + t];
+                gp[r] = pre[(r * SLOTS + kSeg + 1) * NT + t];
+            }
         }
-        if (b + 1 < b_end) prefetch(b + 1);
+        if (b + NR < b_end) prefetch(b + NR);
 
         // ---- compact right-hand side (order 6: the A^-1 part; g keeps the source for T^-1)
-        if constexpr (SRC == 2) {
 #pragma unroll
-            for (int k = 0; k < kSeg; k++) v[k] = cscale(v[k], sp.h2);
-        } else if constexpr (SRC == 4 || SRC == 6) {
-            double2 prev = gm;
+        for (int r = 0; r < NR; r++) {
+            if constexpr (SRC == 2) {
 #pragma unroll
-            for (int k = 0; k < kSeg; k++) {
-                const double2 gk = v[k], nx = (k == kSeg - 1) ? gp : v[k + 1];
-                const double2 d2 = make_double2(fma(-2.0, gk.x, prev.x + nx.x), fma(-2.0, gk.y, prev.y + nx.y));
-                prev = gk;
-                if constexpr (SRC == 6) g[k] = gk;
-                v[k] = zfma(make_double2(c2 * d2.x, c2 * d2.y), c1, gk); // c2 D2 g + c1 g
+                for (int k = 0; k < kSeg; k++) v[r][k] = cscale(v[r][k], sp.h2);
+            } else if constexpr (SRC == 4 || SRC == 6) {
+                double2 prev = gm[r];
+#pragma unroll
+                for (int k = 0; k < kSeg; k++) {
+                    const double2 gk = v[r][k], nx = (k == kSeg - 1) ? gp[r] : v[r][k + 1];
+                    const double2 d2 = make_double2(fma(-2.0, gk.x, prev.x + nx.x), fma(-2.0, gk.y, prev.y + nx.y));
+                    prev = gk;
+                    if constexpr (SRC == 6) g[r][k] = gk;
+                    v[r][k] = zfma(make_double2(c2 * d2.x, c2 * d2.y), c1, gk); // c2 D2 g + c1 g
+                }
             }
         }
 
         // ---- forward elimination: local sweeps from a zero entering value
-        double2 yh = zero, zh = zero;
+        double2 yh[NR], zh[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++) { yh[r] = zero; zh[r] = zero; }
 #pragma unroll
         for (int k = 0; k < kSeg; k++) {
-            yh = zfms(v[k], LF(k), yh);
-            if constexpr (SRC == 6) zh = make_double2(fma(-PL(k), zh.x, g[k].x), fma(-PL(k), zh.y, g[k].y));
-        }
-        double2 Bf = sym_warp_scan<CW, true>(yh, tabF + t, NT, sl);
-        double2 bf = zero;
-        if constexpr (SRC == 6) bf = sym_warp_scan<CW, true>(zh, ttF + t, NT, sl);
-        double2 Bfe = shfl_up2(Bf, CW), bfe = zero;
-        if constexpr (SRC == 6) bfe = shfl_up2(bf, CW);
-        if (sl == 0) { Bfe = zero; bfe = zero; }
-        if (sl == SPW - 1) {
-            sm.BwF[w][c] = Bf;
-            if constexpr (SRC == 6) sm.bwF[w][c] = bf;
-        }
-        __syncthreads();
-        if (t < CW) {
-            double2 E = zero;
+            const double2 l = LF(k);
 #pragma unroll
-            for (int x = 0; x < NW; x++) {
-                sm.EF[x][t] = E;
-                E = zfma(sm.BwF[x][t], sm.AwF[x][t], E);
-            }
-        } else if (SRC == 6 && t >= 32 && t < 32 + CW) {
-            double2 E = zero;
-#pragma unroll
-            for (int x = 0; x < NW; x++) {
-                sm.eF[x][t - 32] = E;
-                E = zaxpy(sm.bwF[x][t - 32], sm.awF[x][t - 32], E);
+            for (int r = 0; r < NR; r++) {
+                yh[r] = zfms(v[r][k], l, yh[r]);
+                if constexpr (SRC == 6)
+                    zh[r] = make_double2(fma(-PL(k), zh[r].x, g[r][k].x), fma(-PL(k), zh[r].y, g[r][k].y));
             }
         }
-        __syncthreads();
-        double2 y = zfma(Bfe, lds_keep(tabF + LOG * NT + t), sm.EF[w][c]);
-        double2 z = zero;
-        if constexpr (SRC == 6) z = zaxpy(bfe, lds_keep(ttF + LOG * NT + t), sm.eF[w][c]);
+        double2 Bfe[NR], bfe[NR];
 #pragma unroll
-        for (int k = 0; k < kSeg; k++) {
-            y = zfms(v[k], LF(k), y);
-            v[k] = y;
+        for (int r = 0; r < NR; r++) {
+            const double2 Bf = sym_warp_scan<CW, true>(yh[r], tabF + t, NT, sl);
+            Bfe[r] = shfl_up2(Bf, CW);
+            bfe[r] = zero;
+            if (sl == SPW - 1) sm.BwF[r][w][c] = Bf;
             if constexpr (SRC == 6) {
-                z = make_double2(fma(-PL(k), z.x, g[k].x), fma(-PL(k), z.y, g[k].y));
-                g[k] = z;
+                const double2 bf = sym_warp_scan<CW, true>(zh[r], ttF + t, NT, sl);
+                bfe[r] = shfl_up2(bf, CW);
+                if (sl == SPW - 1) sm.bwF[r][w][c] = bf;
+            }
+            if (sl == 0) { Bfe[r] = zero; bfe[r] = zero; }
+        }
+        __syncthreads();
+        if (t < CW * NR) {
+            const int r = t / CW, cc = t % CW;
+            double2   E = zero;
+#pragma unroll
+            for (int x = 0; x < NW; x++) {
+                sm.EF[r][x][cc] = E;
+                E = zfma(sm.BwF[r][x][cc], sm.AwF[x][cc], E);
+            }
+        } else if (SRC == 6 && t >= 128 && t < 128 + CW * NR) {
+            const int r = (t - 128) / CW, cc = (t - 128) % CW;
+            double2   E = zero;
+#pragma unroll
+            for (int x = 0; x < NW; x++) {
+                sm.eF[r][x][cc] = E;
+                E = zaxpy(sm.bwF[r][x][cc], sm.awF[x][cc], E);
+            }
+        }
+        __syncthreads();
+        {
+            const double2 AeF = lds_keep(tabF + LOG * NT + t);
+            double        aeF = 0.0;
+            if constexpr (SRC == 6) aeF = lds_keep(ttF + LOG * NT + t);
+            double2 y[NR], z[NR];
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                y[r] = zfma(Bfe[r], AeF, sm.EF[r][w][c]);
+                z[r] = zero;
+                if constexpr (SRC == 6) z[r] = zaxpy(bfe[r], aeF, sm.eF[r][w][c]);
+            }
+#pragma unroll
+            for (int k = 0; k < kSeg; k++) {
+                const double2 l = LF(k);
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    y[r] = zfms(v[r][k], l, y[r]);
+                    v[r][k] = y[r];
+                    if constexpr (SRC == 6) {
+                        z[r] = make_double2(fma(-PL(k), z[r].x, g[r][k].x), fma(-PL(k), z[r].y, g[r][k].y));
+                        g[r][k] = z[r];
+                    }
+                }
             }
         }
 
         // ---- back substitution x_r = ui_r (y_r - s x_{r+1});  Pade: w_r = pu_r (z_r - w_{r+1})
-        double2 xh = zero, wh = zero;
+        double2 xh[NR], wh[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++) { xh[r] = zero; wh[r] = zero; }
 #pragma unroll
         for (int k = kSeg - 1; k >= 0; k--) {
-            xh = cmul(ui[k], zfms(v[k], s, xh));
-            if constexpr (SRC == 6) wh = make_double2(PU(k) * (g[k].x - wh.x), PU(k) * (g[k].y - wh.y));
-        }
-        double2 Bb = sym_warp_scan<CW, false>(xh, tabB + t, NT, sl);
-        double2 bb = zero;
-        if constexpr (SRC == 6) bb = sym_warp_scan<CW, false>(wh, ttB + t, NT, sl);
-        double2 Bbe = shfl_down2(Bb, CW), bbe = zero;
-        if constexpr (SRC == 6) bbe = shfl_down2(bb, CW);
-        if (sl == SPW - 1) { Bbe = zero; bbe = zero; }
-        if (sl == 0) {
-            sm.BwB[w][c] = Bb;
-            if constexpr (SRC == 6) sm.bwB[w][c] = bb;
-        }
-        __syncthreads();
-        if (t < CW) {
-            double2 E = zero;
 #pragma unroll
-            for (int x = NW - 1; x >= 0; x--) {
-                sm.EB[x][t] = E;
-                E = zfma(sm.BwB[x][t], sm.AwB[x][t], E);
-            }
-        } else if (SRC == 6 && t >= 32 && t < 32 + CW) {
-            double2 E = zero;
-#pragma unroll
-            for (int x = NW - 1; x >= 0; x--) {
-                sm.eB[x][t - 32] = E;
-                E = zaxpy(sm.bwB[x][t - 32], sm.awB[x][t - 32], E);
+            for (int r = 0; r < NR; r++) {
+                xh[r] = cmul(ui[k], zfms(v[r][k], s, xh[r]));
+                if constexpr (SRC == 6)
+                    wh[r] = make_double2(PU(k) * (g[r][k].x - wh[r].x), PU(k) * (g[r][k].y - wh[r].y));
             }
         }
-        __syncthreads();
-        double2 xx = zfma(Bbe, lds_keep(tabB + LOG * NT + t), sm.EB[w][c]);
-        double2 ww = zero;
-        if constexpr (SRC == 6) ww = zaxpy(bbe, lds_keep(ttB + LOG * NT + t), sm.eB[w][c]);
+        double2 Bbe[NR], bbe[NR];
 #pragma unroll
-        for (int k = kSeg - 1; k >= 0; k--) {
-            xx = cmul(ui[k], zfms(v[k], s, xx));
-            v[k] = xx;
+        for (int r = 0; r < NR; r++) {
+            const double2 Bb = sym_warp_scan<CW, false>(xh[r], tabB + t, NT, sl);
+            Bbe[r] = shfl_down2(Bb, CW);
+            bbe[r] = zero;
+            if (sl == 0) sm.BwB[r][w][c] = Bb;
             if constexpr (SRC == 6) {
-                ww = make_double2(PU(k) * (g[k].x - ww.x), PU(k) * (g[k].y - ww.y));
-                v[k] = zfma(v[k], cT, ww);
+                const double2 bb = sym_warp_scan<CW, false>(wh[r], ttB + t, NT, sl);
+                bbe[r] = shfl_down2(bb, CW);
+                if (sl == 0) sm.bwB[r][w][c] = bb;
+            }
+            if (sl == SPW - 1) { Bbe[r] = zero; bbe[r] = zero; }
+        }
+        __syncthreads();
+        if (t < CW * NR) {
+            const int r = t / CW, cc = t % CW;
+            double2   E = zero;
+#pragma unroll
+            for (int x = NW - 1; x >= 0; x--) {
+                sm.EB[r][x][cc] = E;
+                E = zfma(sm.BwB[r][x][cc], sm.AwB[x][cc], E);
+            }
+        } else if (SRC == 6 && t >= 128 && t < 128 + CW * NR) {
+            const int r = (t - 128) / CW, cc = (t - 128) % CW;
+            double2   E = zero;
+#pragma unroll
+            for (int x = NW - 1; x >= 0; x--) {
+                sm.eB[r][x][cc] = E;
+                E = zaxpy(sm.bwB[r][x][cc], sm.awB[x][cc], E);
+            }
+        }
+        __syncthreads();
+        {
+            const double2 AeB = lds_keep(tabB + LOG * NT + t);
+            double        aeB = 0.0;
+            if constexpr (SRC == 6) aeB = lds_keep(ttB + LOG * NT + t);
+            double2 x[NR], ww[NR];
+#pragma unroll
+            for (int r = 0; r < NR; r++) {
+                x[r] = zfma(Bbe[r], AeB, sm.EB[r][w][c]);
+                ww[r] = zero;
+                if constexpr (SRC == 6) ww[r] = zaxpy(bbe[r], aeB, sm.eB[r][w][c]);
+            }
+#pragma unroll
+            for (int k = kSeg - 1; k >= 0; k--) {
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    x[r] = cmul(ui[k], zfms(v[r][k], s, x[r]));
+                    v[r][k] = x[r];
+                    if constexpr (SRC == 6) {
+                        ww[r] = make_double2(PU(k) * (g[r][k].x - ww[r].x), PU(k) * (g[r][k].y - ww[r].y));
+                        v[r][k] = zfma(v[r][k], cT, ww[r]);
+                    }
+                }
             }
         }
 
-        double2 *dst = out + (long)b * field + off0;
 #pragma unroll
-        for (int k = 0; k < kSeg; k++)
-            if (live && r0 + k < rows) dst[(long)k * row_stride] = v[k];
+        for (int r = 0; r < NR; r++) {
+            if (b + r >= b_end) break;
+            double2 *dst = out + (long)(b + r) * field + off0;
+#pragma unroll
+            for (int k = 0; k < kSeg; k++)
+                if (live && r0 + k < rows) dst[(long)k * row_stride] = v[r][k];
+        }
     }
 }
 
@@ -859,17 +931,17 @@ __device__ __forceinline__ M sym_scan_table(M a, M *tab, int NT_, int sl, M one)
     return a;
 }
 
-template <int SRC, int NT, int CW, int MINB>
+template <int SRC, int NT, int CW, int MINB, int NR>
 __global__ void __launch_bounds__(NT, MINB)
     k_line_solve_sym(const double2 *__restrict__ in, double2 *__restrict__ out, int lines, int rows, long row_stride,
                      long field, int batch, int rb, const double2 *__restrict__ Pv, const double2 *__restrict__ subt,
                      const double2 *__restrict__ diagt, int prow, const double *__restrict__ mu, SymParams sp) {
     constexpr int NW = NT / 32, SPW = 32 / CW, LOG = ilog2_t<SPW>();
     constexpr int HALO = (SRC == 4 || SRC == 6) ? 1 : 0;
-    __shared__ SymSmem<NW, CW> sm;
+    __shared__ SymSmem<NW, CW, NR> sm;
     extern __shared__ double2 dyn[];
-    double2 *pre = dyn;                                 // [kSeg + 2][NT]
-    double2 *tabF = pre + (kSeg + 2) * NT;              // [LOG + 1][NT]
+    double2 *pre = dyn;                                 // [NR][kSeg + 2][NT]
+    double2 *tabF = pre + NR * (kSeg + 2) * NT;         // [LOG + 1][NT]
     double2 *tabB = tabF + (LOG + 1) * NT;              // [LOG + 1][NT]
     double  *ttF = reinterpret_cast<double *>(tabB + (LOG + 1) * NT); // [LOG + 1][NT] (order 6)
     double  *ttB = ttF + (LOG + 1) * NT;
@@ -967,14 +1039,30 @@ __global__ void __launch_bounds__(NT, MINB)
     // warps whose rows all lie in [9, rows) use the constant Pade factors
     const bool tint = (w * SPW * kSeg >= 9) && ((w + 1) * SPW * kSeg <= rows);
     if (SRC == 6 && tint)
-        sym_chunk<SRC, NT, CW, true>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0, sl, w, c, Lr,
+        sym_chunk<SRC, NT, CW, true, NR>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0, sl, w, c, Lr,
                                      ui, ui_in, s, c1, c2, cT, sm, pre, tabF, tabB, ttF, ttB, sp);
     else
-        sym_chunk<SRC, NT, CW, false>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0, sl, w, c, Lr,
+        sym_chunk<SRC, NT, CW, false, NR>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0, sl, w, c, Lr,
                                       ui, ui_in, s, c1, c2, cT, sm, pre, tabF, tabB, ttF, ttB, sp);
 }
 
-template <int SRC, int CW, int MINB>
+// Right-hand sides per CTA: the chunk whose grid has the smallest wave-quantised cost,
+//   ceil(CTAs / resident CTAs) * (rb + 1),
+// counting the per-chunk set-up (factors and scan tables) as about one right-hand side.
+static int pick_rb(long groups, int batch, int resident, int nr) {
+    int  best = nr, rb = nr;
+    long best_cost = -1;
+    for (; ; rb *= 2) {
+        const int  r = rb < batch ? rb : batch;
+        const long ctas = groups * ((batch + r - 1) / r);
+        const long cost = ((ctas + resident - 1) / resident) * (long)(r + 1);
+        if (best_cost < 0 || cost < best_cost) { best_cost = cost; best = r; }
+        if (rb >= batch) break;
+    }
+    return best;
+}
+
+template <int SRC, int CW, int MINB, int NR>
 static int launch_sym_t(Plan *p, const double2 *in, double2 *out, int batch) {
     constexpr int NT = 256, SPW = 32 / CW, LOG = ilog2_t<SPW>();
     SymParams sp;
@@ -985,33 +1073,37 @@ static int launch_sym_t(Plan *p, const double2 *in, double2 *out, int batch) {
     sp.uinf = p->pade_uinf;
     sp.pl = p->pade_l;
     sp.pu = p->pade_u;
-    const int shm = (int)(sizeof(double2) * ((kSeg + 2) * NT + 2 * (LOG + 1) * NT) +
+    const int shm = (int)(sizeof(double2) * (NR * (kSeg + 2) * NT + 2 * (LOG + 1) * NT) +
                           (SRC == 6 ? sizeof(double) * 2 * (LOG + 1) * NT : 0));
-    HH_CUDA(cudaFuncSetAttribute(k_line_solve_sym<SRC, NT, CW, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
+    HH_CUDA(cudaFuncSetAttribute(k_line_solve_sym<SRC, NT, CW, MINB, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 shm));
     const long groups = (p->lines + CW - 1) / CW;
-    int rb = 1;
-    while (rb < batch && groups * ((batch + 2 * rb - 1) / (2 * rb)) >= 2L * MINB * 148) rb *= 2;
+    int blocks_per_sm = 0, dev = 0, sms = 148;
+    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_line_solve_sym<SRC, NT, CW, MINB, NR>, NT,
+                                                          shm));
+    HH_CUDA(cudaGetDevice(&dev));
+    HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int rb = pick_rb(groups, batch, std::max(1, blocks_per_sm) * sms, NR);
     const int chunks = (batch + rb - 1) / rb;
     dim3 grid((unsigned)groups, (unsigned)chunks);
-    k_line_solve_sym<SRC, NT, CW, MINB><<<grid, NT, shm, p->ctx->stream>>>(in, out, p->lines, p->rows, p->row_stride,
-                                                                     p->field, batch, rb, p->Pv, p->subt, p->diagt,
-                                                                     p->prow, p->mu, sp);
+    k_line_solve_sym<SRC, NT, CW, MINB, NR><<<grid, NT, shm, p->ctx->stream>>>(
+        in, out, p->lines, p->rows, p->row_stride, p->field, batch, rb, p->Pv, p->subt, p->diagt, p->prow, p->mu, sp);
     HH_CUDA(cudaGetLastError());
     p->ctx->launches++;
     return HH_OK;
 }
 
-template <int SRC, int MINB> static int launch_sym_src(Plan *p, const double2 *in, double2 *out, int batch) {
+template <int SRC, int MINB, int NR> static int launch_sym_src(Plan *p, const double2 *in, double2 *out, int batch) {
     // segments per line: a power of two P >= rows / kSeg with 8 <= P <= 256 (CW = 256 / P lines per CTA)
     int P = 8;
     while (P * kSeg < p->rows) P <<= 1;
     switch (P) {
-    case 8: return launch_sym_t<SRC, 32, MINB>(p, in, out, batch);
-    case 16: return launch_sym_t<SRC, 16, MINB>(p, in, out, batch);
-    case 32: return launch_sym_t<SRC, 8, MINB>(p, in, out, batch);
-    case 64: return launch_sym_t<SRC, 4, MINB>(p, in, out, batch);
-    case 128: return launch_sym_t<SRC, 2, MINB>(p, in, out, batch);
-    case 256: return launch_sym_t<SRC, 1, MINB>(p, in, out, batch);
+    case 8: return launch_sym_t<SRC, 32, MINB, 1>(p, in, out, batch); // per-RHS scan arrays would not fit
+    case 16: return launch_sym_t<SRC, 16, MINB, NR>(p, in, out, batch);
+    case 32: return launch_sym_t<SRC, 8, MINB, NR>(p, in, out, batch);
+    case 64: return launch_sym_t<SRC, 4, MINB, NR>(p, in, out, batch);
+    case 128: return launch_sym_t<SRC, 2, MINB, NR>(p, in, out, batch);
+    case 256: return launch_sym_t<SRC, 1, MINB, NR>(p, in, out, batch);
     default: set_error("symmetric line solve: %d rows", p->rows); return HH_ERR_UNSUPPORTED;
     }
 }
@@ -1020,13 +1112,22 @@ bool sym_solve_supported(const Plan *p, int src_order) {
     return p->sym && p->rows <= 256 * kSeg && (src_order != 6 || (p->pf_ok && p->pade_l));
 }
 
+// Variants of the symmetric kernel: 2 = two CTAs per SM, 3 = one CTA per SM (no register cap),
+// 4 = one CTA per SM with two right-hand sides per pass.
+template <int SRC> static int launch_sym_variant(Plan *p, const double2 *in, double2 *out, int batch) {
+    switch (p->variant) {
+    case 3: return launch_sym_src<SRC, 1, 1>(p, in, out, batch);
+    case 4: return launch_sym_src<SRC, 1, 2>(p, in, out, batch);
+    default: return launch_sym_src<SRC, 2, 1>(p, in, out, batch);
+    }
+}
+
 int launch_line_solve_sym(Plan *p, const double2 *in, double2 *out, int batch, int src_order) {
-    // variant 3: order 6 with one 256-thread CTA per SM and no register cap (no spills)
     switch (src_order) {
-    case 0: return launch_sym_src<0, 2>(p, in, out, batch);
-    case 2: return launch_sym_src<2, 2>(p, in, out, batch);
-    case 4: return launch_sym_src<4, 2>(p, in, out, batch);
-    case 6: return p->variant == 3 ? launch_sym_src<6, 1>(p, in, out, batch) : launch_sym_src<6, 2>(p, in, out, batch);
+    case 0: return launch_sym_variant<0>(p, in, out, batch);
+    case 2: return launch_sym_variant<2>(p, in, out, batch);
+    case 4: return launch_sym_variant<4>(p, in, out, batch);
+    case 6: return launch_sym_variant<6>(p, in, out, batch);
     default: set_error("source operator order %d", src_order); return HH_ERR_INVALID;
     }
 }
