@@ -27,6 +27,8 @@
 // double costs four shuffles per hop.
 #include "hh_internal.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <math.h>
 
 #include <algorithm>
@@ -167,6 +169,21 @@ __device__ __forceinline__ bool mbar_wait0(uint64_t *bar) {
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
             : "=r"(done)
             : "r"(a)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// bounded wait on an mbarrier phase; false if it did not complete within the budget
+__device__ __forceinline__ bool mbar_wait_parity(uint64_t *bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (long it = 0; it < (1L << 26); it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
             : "memory");
         if (done) return true;
     }
@@ -354,129 +371,277 @@ __global__ void __launch_bounds__(DstGeom<M>::NT)
     }
 }
 
-// ------------------------------------------ one warp per line: M = 1024 rows ------
-// The same transform for contiguous rows of length N = 1023 with one warp per line and M = 32 x 32:
-//   lane b loads x_j and the mirror x_{M-j} for j = b + 32 q straight from global memory
-//   (coalesced), forms y_j in registers, runs a 32-point DFT over q, twiddles, and exchanges
-//   through one padded transpose; the second 32-point DFT leaves Y_{b + 32 k2} in lane b.
-//   Post-processing runs on blocks (lane t owns k in [16t, 16t + 16)), so the prefix sum of the
-//   odd outputs is a sequential sum plus one warp scan; the outputs go back through shared
-//   memory so that the global stores are coalesced.
-// Shared-memory traffic per point: transpose (write + read), Y (write + read), S (write + read);
-// the staged design above makes about twice as many passes.
+// ------------------------------- persistent warps, one line per TL lanes (rows) ------
+// The same transform for contiguous rows, M = TL x R with TL = 8, 16 or 32 lanes per line
+// (32/TL lines per warp) and R values per lane:
+//   lane l of a line holds x_j and the mirror x_{M-j} for j = l + TL q (read from the line
+//   buffer that the TMA filled), forms y_j in registers, runs an R-point DFT over q, twiddles by
+//   W_M^{l k1} and exchanges through one padded transpose; TL-point DFTs over l then leave
+//   Y_{k1 + R k2} for k1 = l + TL i in the lane.
+//   Post-processing runs on blocks (lane l owns k in [KB l, KB l + KB), KB = M/(2 TL)), so the
+//   prefix sum of the odd outputs is a sequential sum plus one scan over the line's lanes; the
+//   outputs go back through the buffer so that the global stores are coalesced.
+// Each warp owns two buffer sets and works through line groups w, w + W, ...: while it
+// transforms one group, the TMA brings in the next.
 
-// sin(pi m / 32), m = 0..16
-__device__ __forceinline__ constexpr double sinpi32(int m) {
-    constexpr double s[17] = {0.0,
+// sin(pi m / 64), m = 0..32
+__device__ __forceinline__ constexpr double sinpi64(int m) {
+    constexpr double s[33] = {0.0,
+                              0.049067674327418014255,
                               0.098017140329560601994,
+                              0.14673047445536175166,
                               0.19509032201612826785,
+                              0.24298017990326388995,
                               0.29028467725446236764,
+                              0.33688985339222005069,
                               0.38268343236508977173,
+                              0.42755509343028209432,
                               0.47139673682599764856,
+                              0.51410274419322172659,
                               0.55557023301960222474,
+                              0.59569930449243334347,
                               0.63439328416364549822,
+                              0.67155895484701840063,
                               0.7071067811865475244,
+                              0.74095112535495909118,
                               0.77301045336273696081,
+                              0.80320753148064490981,
                               0.83146961230254523708,
+                              0.8577286100002720699,
                               0.88192126434835502971,
+                              0.90398929312344333159,
                               0.92387953251128675613,
+                              0.94154406518302077841,
                               0.95694033573220886494,
+                              0.9700312531945439926,
                               0.98078528040323044913,
+                              0.98917650996478097345,
                               0.99518472667219688624,
+                              0.99879545620517239271,
                               1.0};
     return s[m];
 }
-// sin(pi q / 32) and cos(pi q / 32) for q = 0..31
-__device__ __forceinline__ constexpr double sin_q32(int q) { return q <= 16 ? sinpi32(q) : sinpi32(32 - q); }
-__device__ __forceinline__ constexpr double cos_q32(int q) { return q <= 16 ? sinpi32(16 - q) : -sinpi32(q - 16); }
+// sin and cos of pi m / 64 for m = 0..63
+__device__ __forceinline__ constexpr double sin_m64(int m) { return m <= 32 ? sinpi64(m) : sinpi64(64 - m); }
+__device__ __forceinline__ constexpr double cos_m64(int m) { return m <= 32 ? sinpi64(32 - m) : -sinpi64(m - 32); }
 
-// v * exp(-2 pi i t / 32), t = 0..15: cos(2 pi t/32) = sin(pi (8 - t)/16) = sinpi32(16 - 2t)
-template <int t> __device__ __forceinline__ double2 tw32_mul(double2 v) {
+// v * exp(-2 pi i t / R), 0 <= t < R/2, R <= 64 (angle pi m / 64 with m = 128 t / R)
+template <int R, int t> __device__ __forceinline__ double2 twr_mul(double2 v) {
+    constexpr int m = t * (128 / R);
     if constexpr (t == 0) return v;
-    else if constexpr (t == 8) return make_double2(v.y, -v.x);
-    else if constexpr (t == 4) {
-        constexpr double r = sinpi32(8);
+    else if constexpr (m == 32) return make_double2(v.y, -v.x);
+    else if constexpr (m == 16) {
+        constexpr double r = sinpi64(16);
         return make_double2((v.x + v.y) * r, (v.y - v.x) * r);
-    } else if constexpr (t == 12) {
-        constexpr double r = sinpi32(8);
+    } else if constexpr (m == 48) {
+        constexpr double r = sinpi64(16);
         return make_double2((v.y - v.x) * r, -(v.x + v.y) * r);
     } else {
-        constexpr double c = t < 8 ? sinpi32(16 - 2 * t) : -sinpi32(2 * t - 16), s = sinpi32(t < 8 ? 2 * t : 32 - 2 * t);
+        constexpr double c = cos_m64(m), s = sin_m64(m);
         return make_double2(fma(v.x, c, v.y * s), fma(v.y, c, -(v.x * s)));
     }
 }
-template <int SPAN, int J> struct Dif32Butterflies {
-    __device__ __forceinline__ static void run(double2 (&v)[32], int start) {
+template <int R, int SPAN, int J> struct DifRB {
+    __device__ __forceinline__ static void run(double2 (&v)[R], int start) {
         if constexpr (J < SPAN) {
             const double2 a = v[start + J], b = v[start + J + SPAN];
             v[start + J] = cadd(a, b);
-            v[start + J + SPAN] = tw32_mul<J * (16 / SPAN)>(csub(a, b));
-            Dif32Butterflies<SPAN, J + 1>::run(v, start);
+            v[start + J + SPAN] = twr_mul<R, J * (R / (2 * SPAN))>(csub(a, b));
+            DifRB<R, SPAN, J + 1>::run(v, start);
         }
     }
 };
-template <int SPAN, int START> struct Dif32Stage {
-    __device__ __forceinline__ static void run(double2 (&v)[32]) {
-        if constexpr (START < 32) {
-            Dif32Butterflies<SPAN, 0>::run(v, START);
-            Dif32Stage<SPAN, START + 2 * SPAN>::run(v);
+template <int R, int SPAN, int START> struct DifRS {
+    __device__ __forceinline__ static void run(double2 (&v)[R]) {
+        if constexpr (START < R) {
+            DifRB<R, SPAN, 0>::run(v, START);
+            DifRS<R, SPAN, START + 2 * SPAN>::run(v);
         }
     }
 };
-template <int SPAN> struct Dif32All {
-    __device__ __forceinline__ static void run(double2 (&v)[32]) {
+template <int R, int SPAN> struct DifRA {
+    __device__ __forceinline__ static void run(double2 (&v)[R]) {
         if constexpr (SPAN >= 1) {
-            Dif32Stage<SPAN, 0>::run(v);
-            Dif32All<SPAN / 2>::run(v);
+            DifRS<R, SPAN, 0>::run(v);
+            DifRA<R, SPAN / 2>::run(v);
         }
     }
 };
-// forward 32-point DFT in registers; X[k] = v[bitrev5(k)]
-__device__ __forceinline__ void dft32(double2 (&v)[32]) { Dif32All<16>::run(v); }
+// forward R-point DFT in registers (R <= 64); X[k] = v[bitrev(k)]
+template <int R> __device__ __forceinline__ void dft_r(double2 (&v)[R]) { DifRA<R, R / 2>::run(v); }
 
-constexpr int kDstWarps = 2;                  // warps per CTA
-constexpr int kDstWarpBuf = 1088;             // double2 per buffer: max(32 x 33, 1024 + 1024/16)
-__host__ __device__ constexpr int hibit(int k) { return k <= 1 ? 0 : 1 + hibit(k >> 1); }
-__host__ __device__ constexpr int t33(int i, int j) { return 33 * i + j; }          // transpose layout
-__host__ __device__ constexpr int p16(int k) { return k + (k >> 4); }               // Y layout
-__host__ __device__ constexpr int o33(int p) { return 33 * (p >> 5) + (p & 31); }   // output layout
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
-// bounded wait on an mbarrier phase; false if it did not complete within the budget
-__device__ __forceinline__ bool mbar_wait_parity(uint64_t *bar, uint32_t parity) {
-    const uint32_t a = smem_u32(bar);
-    for (long it = 0; it < (1L << 26); it++) {
-        uint32_t done;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(done)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (done) return true;
+template <int M> struct WCfg;
+template <> struct WCfg<1024> { static constexpr int TL = 32, R = 32, WPC = 2; };
+template <> struct WCfg<512>  { static constexpr int TL = 16, R = 32, WPC = 2; };
+template <> struct WCfg<256>  { static constexpr int TL = 16, R = 16, WPC = 4; };
+template <> struct WCfg<128>  { static constexpr int TL = 8,  R = 16, WPC = 4; };
+template <> struct WCfg<64>   { static constexpr int TL = 8,  R = 8,  WPC = 4; };
+
+template <int M> struct WGeom {
+    static constexpr int TL = WCfg<M>::TL, R = WCfg<M>::R, WPC = WCfg<M>::WPC;
+    static constexpr int LPW = 32 / TL, KB = M / (2 * TL);
+    // one line's buffer: raw line, transpose [R][TL + 1], Y (k + k/KB), outputs ((2KB + 1) per 2KB)
+    static constexpr int BUF = cmax(R * (TL + 1), cmax(M + M / KB, M + M / (2 * KB))) + 1;
+    static constexpr int WARP_ELEMS = 2 * LPW * BUF; // two buffer sets per warp
+    static constexpr int SMEM = 16 * WPC + 16 * WARP_ELEMS * WPC;
+};
+
+// Per-lane constants of the transform: sin, cos(pi l / M) and the twiddles W_M^{l a} (a < 8),
+// W_M^{8 l b} (b < R/8).
+template <int M> struct WConst {
+    static constexpr int NB = WCfg<M>::R / 8 > 0 ? WCfg<M>::R / 8 : 1;
+    double               sb, cb;
+    double2              twa[8], twb[NB];
+    __device__ __forceinline__ void load(int l, const double2 *__restrict__ tw, const double *__restrict__ sn) {
+        sb = __ldg(sn + l);
+        cb = __ldg(sn + M / 2 - l);
+#pragma unroll
+        for (int a = 0; a < 8; a++) twa[a] = __ldg(tw + ((l * a) & (M - 1)));
+#pragma unroll
+        for (int b = 0; b < NB; b++) twb[b] = __ldg(tw + ((8 * l * b) & (M - 1)));
     }
-    return false;
+    // re-formed for every line: an empty asm hides them from loop-invariant hoisting, which would
+    // otherwise pin every derived sine and twiddle in registers
+    __device__ __forceinline__ void launder() {
+        asm volatile("" : "+d"(sb), "+d"(cb));
+#pragma unroll
+        for (int a = 0; a < 8; a++) asm volatile("" : "+d"(twa[a].x), "+d"(twa[a].y));
+#pragma unroll
+        for (int b = 0; b < NB; b++) asm volatile("" : "+d"(twb[b].x), "+d"(twb[b].y));
+    }
+};
+
+// inclusive scan over the TL lanes of a line: contiguous lanes (rows kernel) or lanes c + LPW l
+// (columns kernel)
+template <int TL, int LPW, bool INTER> __device__ __forceinline__ double2 line_scan(double2 x, int l) {
+#pragma unroll
+    for (int off = 1; off < TL; off <<= 1) {
+        double ox, oy;
+        if constexpr (INTER) {
+            ox = __shfl_up_sync(0xffffffffu, x.x, off * LPW);
+            oy = __shfl_up_sync(0xffffffffu, x.y, off * LPW);
+        } else {
+            ox = __shfl_up_sync(0xffffffffu, x.x, off, TL);
+            oy = __shfl_up_sync(0xffffffffu, x.y, off, TL);
+        }
+        if (l >= off) { x.x += ox; x.y += oy; }
+    }
+    return x;
 }
 
-// Persistent warps: warp w of the grid transforms lines w, w + W, w + 2W, ... (W warps in all),
-// each line (plane = g / nlines, line = g % nlines) at in + plane*in_plane + line*in_ld with x_1..x_N
-// at offsets 0..N-1, and likewise for the output.  Each warp owns two line buffers: while it
-// transforms one line, the TMA brings in its next.  in and out may be the same buffer.
-__global__ void __launch_bounds__(32 * kDstWarps, 3)
-    k_dst1_w1024(const double2 *in, double2 *out, long nlines, long nplanes, long in_ld, long out_ld, long in_plane,
-                 long out_plane, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
-    constexpr int      M = 1024, N = M - 1;
-    constexpr uint32_t kBytes = N * 16;
+// The transform of one line by its TL lanes.  xload(j) returns x_j (1 <= j <= N) from wherever
+// the line was staged; `buf` is the line's exchange area (BUF elements, may be that staging
+// area: every x_j is read before the first write).  On return the outputs sit in buf at
+// (2KB + 1)(p / 2KB) + p % 2KB for output offset p.
+template <int M, bool INTER, typename XLoad>
+__device__ __forceinline__ void w_transform(XLoad xload, double2 *buf, int l, bool live, WConst<M> &K) {
+    using G = WGeom<M>;
+    constexpr int TL = G::TL, R = G::R, LPW = G::LPW, KB = G::KB, K2 = 2 * KB;
+    const double2 zero = make_double2(0.0, 0.0);
+    K.launder();
+
+    // ---- y_j = sin(pi j/M)(x_j + x_{M-j}) + (x_j - x_{M-j})/2,  j = l + TL q
+    double2 v[R];
+#pragma unroll
+    for (int q = 0; q < R; q++) {
+        const int j = l + TL * q;
+        double2   a = zero, m = zero;
+        if (live && (q > 0 || l > 0)) {
+            a = xload(j);
+            m = xload(M - j);
+        }
+        const double s = fma(K.sb, cos_m64(q * (64 / R)), K.cb * sin_m64(q * (64 / R))); // sin(pi j / M)
+        v[q] = make_double2(fma(s, a.x + m.x, 0.5 * (a.x - m.x)), fma(s, a.y + m.y, 0.5 * (a.y - m.y)));
+    }
+    __syncwarp(); // staged input consumed
+
+    // ---- R-point DFTs over q, twiddle W_M^{l k1}, transpose [k1][l]
+    dft_r<R>(v);
+#pragma unroll
+    for (int k1 = 0; k1 < R; k1++)
+        buf[k1 * (TL + 1) + l] = k1 ? cmul(v[bitrev_c<R>(k1)], cmul(K.twa[k1 & 7], K.twb[k1 >> 3])) : v[0];
+    __syncwarp();
+    double2 w2[R / TL][TL]; // lane l takes k1 = l + TL i with all TL values of l'
+#pragma unroll
+    for (int i = 0; i < R / TL; i++)
+#pragma unroll
+        for (int lp = 0; lp < TL; lp++) w2[i][lp] = buf[(l + TL * i) * (TL + 1) + lp];
+    __syncwarp();
+
+    // ---- TL-point DFTs over l': Y_{k1 + R k2} = w2[i][bitrev(k2)]
+#pragma unroll
+    for (int i = 0; i < R / TL; i++) {
+        dft_r<TL>(w2[i]);
+#pragma unroll
+        for (int k2 = 0; k2 < TL; k2++) {
+            const int k = l + TL * i + R * k2;
+            buf[k + k / KB] = w2[i][bitrev_c<TL>(k2)];
+        }
+    }
+    __syncwarp();
+
+    // ---- post-processing on blocks k = KB l + u
+    double2 cs[KB], ev[KB];
+    double2 run = zero;
+#pragma unroll
+    for (int u = 0; u < KB; u++) {
+        const int     k = KB * l + u;
+        const double2 yk = buf[k + k / KB];
+        if (k == 0) {
+            cs[u] = make_double2(0.5 * yk.x, 0.5 * yk.y);
+            ev[u] = zero;
+        } else {
+            const int     km = M - k;
+            const double2 ym = buf[km + km / KB];
+            cs[u] = make_double2(0.5 * (yk.x + ym.x), 0.5 * (yk.y + ym.y));
+            ev[u] = make_double2(0.5 * (ym.y - yk.y), -0.5 * (ym.x - yk.x)); // (Y_{M-k} - Y_k)/(2i)
+        }
+        run = cadd(run, cs[u]);
+        cs[u] = run;
+    }
+    const double2 pre = csub(line_scan<TL, LPW, INTER>(run, l), run);
+    const double  coef = sqrt(2.0 / M);
+    __syncwarp(); // every read of Y is done
+#pragma unroll
+    for (int u = 0; u < KB; u++) {
+        const int k = KB * l + u, po = 2 * k, pe = 2 * k - 1;
+        buf[(K2 + 1) * (po / K2) + po % K2] = cscale(cadd(pre, cs[u]), coef); // S_{2k+1} at 2k
+        if (k > 0) buf[(K2 + 1) * (pe / K2) + pe % K2] = cscale(ev[u], coef); // S_{2k}   at 2k-1
+    }
+    __syncwarp();
+}
+
+// ---- rows: lines g = 0 .. nlines*nplanes-1 at in + (g / nlines) in_plane + (g % nlines) in_ld
+// with x_1..x_N at offsets 0..N-1, likewise for the output; in and out may be the same buffer.
+template <int M>
+__global__ void __launch_bounds__(32 * WCfg<M>::WPC, 3)
+    k_dst1_w(const double2 *in, double2 *out, long nlines, long nplanes, long in_ld, long out_ld, long in_plane,
+             long out_plane, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
+    using G = WGeom<M>;
+    constexpr int      TL = G::TL, LPW = G::LPW, KB = G::KB, BUF = G::BUF, N = M - 1, K2 = 2 * KB;
+    constexpr uint32_t kLineBytes = N * 16;
     extern __shared__ __align__(128) unsigned char dsm[];
     const int  lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+    const int  c = lane / TL, l = lane % TL; // line of the warp's group, lane within the line
     uint64_t  *bar = reinterpret_cast<uint64_t *>(dsm) + 2 * wq;
-    double2   *bufs = reinterpret_cast<double2 *>(dsm + 16 * kDstWarps) + 2 * wq * kDstWarpBuf;
+    double2   *sets = reinterpret_cast<double2 *>(dsm + 16 * G::WPC) + wq * G::WARP_ELEMS;
     const long total = nlines * nplanes;
-    const long stride = (long)gridDim.x * kDstWarps;
-    const long g0 = (long)blockIdx.x * kDstWarps + wq;
-    if (g0 >= total) return; // whole warp
-    const double2 zero = make_double2(0.0, 0.0);
+    const long groups = (total + LPW - 1) / LPW;
+    const long stride = (long)gridDim.x * G::WPC;
+    const long g0 = (long)blockIdx.x * G::WPC + wq;
+    if (g0 >= groups) return; // whole warp
 
     auto src_of = [&](long g) { return in + (g / nlines) * in_plane + (g % nlines) * in_ld; };
     auto dst_of = [&](long g) { return out + (g / nlines) * out_plane + (g % nlines) * out_ld; };
+    // lane 0: bring in line group `grp` to buffer set `s`
+    auto fetch = [&](long grp, int s) {
+        const long first = grp * LPW;
+        const int  nl = (int)((total - first) < LPW ? (total - first) : LPW);
+        mbar_expect_tx(&bar[s], (uint32_t)nl * kLineBytes);
+        for (int x = 0; x < nl; x++) tma_bulk_load(sets + (s * LPW + x) * BUF, src_of(first + x), kLineBytes, &bar[s]);
+    };
     if (lane == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
@@ -484,126 +649,165 @@ __global__ void __launch_bounds__(32 * kDstWarps, 3)
     }
     __syncwarp();
     if (lane == 0) {
-        mbar_expect_tx(&bar[0], kBytes);
-        tma_bulk_load(bufs, src_of(g0), kBytes, &bar[0]);
-        if (g0 + stride < total) {
-            mbar_expect_tx(&bar[1], kBytes);
-            tma_bulk_load(bufs + kDstWarpBuf, src_of(g0 + stride), kBytes, &bar[1]);
-        }
+        fetch(g0, 0);
+        if (g0 + stride < groups) fetch(g0 + stride, 1);
     }
+    WConst<M> K;
+    K.load(l, tw, sn);
 
-    // per-lane constants: sin, cos(pi lane / M) and the twiddles W_M^{lane a}, W_M^{8 lane b}
-    const double sb = __ldg(sn + lane), cb = __ldg(sn + M / 2 - lane);
-    double2      twa[8], twb[4];
-#pragma unroll
-    for (int a = 0; a < 8; a++) twa[a] = __ldg(tw + ((lane * a) & (M - 1)));
-#pragma unroll
-    for (int b = 0; b < 4; b++) twb[b] = __ldg(tw + ((8 * lane * b) & (M - 1)));
-    const double coef = sqrt(2.0 / M);
-
-    int  i = 0;
+    int  it = 0;
     long failed = -1;
-    for (long g = g0; g < total; g += stride, i++) {
-        double2 *buf = bufs + (i & 1) * kDstWarpBuf;
-        if (!mbar_wait_parity(&bar[i & 1], (i >> 1) & 1)) {
+    for (long grp = g0; grp < groups; grp += stride, it++) {
+        const int s = it & 1;
+        double2  *buf = sets + (s * LPW + c) * BUF;
+        const long line = grp * LPW + c;
+        const bool live = line < total;
+        if (!mbar_wait_parity(&bar[s], (it >> 1) & 1)) {
             if (lane == 0) atomicExch(err, 1);
-            failed = g;
+            failed = grp;
             break;
         }
-
-        // The per-lane sines and twiddles are re-formed for every line: an empty asm hides their
-        // inputs from loop-invariant hoisting, which would otherwise pin ~90 registers.
-        double sbl = sb, cbl = cb;
-        asm volatile("" : "+d"(sbl), "+d"(cbl));
+        w_transform<M, false>([&](int j) { return buf[j - 1]; }, buf, l, live, K);
+        if (live) {
+            double2 *dst = dst_of(line);
 #pragma unroll
-        for (int a = 0; a < 8; a++) asm volatile("" : "+d"(twa[a].x), "+d"(twa[a].y));
-#pragma unroll
-        for (int b = 0; b < 4; b++) asm volatile("" : "+d"(twb[b].x), "+d"(twb[b].y));
-
-        // ---- y_j = sin(pi j/M)(x_j + x_{M-j}) + (x_j - x_{M-j})/2,  j = lane + 32 q
-        double2 v[32];
-#pragma unroll
-        for (int q = 0; q < 32; q++) {
-            const int j = lane + 32 * q;
-            double2   a = zero, m = zero;
-            if (q > 0 || lane > 0) {
-                a = buf[j - 1];
-                m = buf[M - j - 1];
+            for (int q = 0; q < M / TL; q++) {
+                const int p = l + TL * q;
+                if (p < N) dst[p] = buf[(K2 + 1) * (p / K2) + p % K2];
             }
-            const double s = fma(sbl, cos_q32(q), cbl * sin_q32(q)); // sin(pi (lane + 32 q) / M)
-            v[q] = make_double2(fma(s, a.x + m.x, 0.5 * (a.x - m.x)), fma(s, a.y + m.y, 0.5 * (a.y - m.y)));
         }
-        __syncwarp(); // the raw line is consumed; the buffer becomes the exchange area
-
-        // ---- 32-point DFTs over q, twiddle W_M^{lane k1}, transpose
-        dft32(v);
-#pragma unroll
-        for (int k1 = 0; k1 < 32; k1++)
-            buf[t33(k1, lane)] = k1 ? cmul(v[bitrev_c<32>(k1)], cmul(twa[k1 & 7], twb[k1 >> 3])) : v[0];
+        // the buffer set is free again: bring in the group after next (every lane orders its
+        // generic-proxy accesses before the asynchronous copy that overwrites them)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncwarp();
-#pragma unroll
-        for (int j1 = 0; j1 < 32; j1++) v[j1] = buf[t33(lane, j1)];
-        __syncwarp();
-
-        // ---- 32-point DFTs over j1: Y_{lane + 32 k2} = v[bitrev(k2)]
-        dft32(v);
-#pragma unroll
-        for (int k2 = 0; k2 < 32; k2++) buf[p16(lane + 32 * k2)] = v[bitrev_c<32>(k2)];
-        __syncwarp();
-
-        // ---- post-processing on blocks k = 16 lane + u
-        double2 cs[16], ev[16];
-        double2 run = zero;
-#pragma unroll
-        for (int u = 0; u < 16; u++) {
-            const int     k = 16 * lane + u;
-            const double2 yk = buf[p16(k)];
-            if (k == 0) {
-                cs[u] = make_double2(0.5 * yk.x, 0.5 * yk.y);
-                ev[u] = zero;
-            } else {
-                const double2 ym = buf[p16(M - k)];
-                cs[u] = make_double2(0.5 * (yk.x + ym.x), 0.5 * (yk.y + ym.y));
-                ev[u] = make_double2(0.5 * (ym.y - yk.y), -0.5 * (ym.x - yk.x)); // (Y_{M-k} - Y_k)/(2i)
-            }
-            run = cadd(run, cs[u]);
-            cs[u] = run;
-        }
-        double2 incl = run;
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const double ox = __shfl_up_sync(0xffffffffu, incl.x, off), oy = __shfl_up_sync(0xffffffffu, incl.y, off);
-            if (lane >= off) { incl.x += ox; incl.y += oy; }
-        }
-        const double2 pre = csub(incl, run);
-        __syncwarp(); // every read of Y is done
-#pragma unroll
-        for (int u = 0; u < 16; u++) {
-            const int k = 16 * lane + u;
-            buf[o33(2 * k)] = cscale(cadd(pre, cs[u]), coef);     // S_{2k+1} at offset 2k
-            if (k > 0) buf[o33(2 * k - 1)] = cscale(ev[u], coef); // S_{2k}   at offset 2k-1
-        }
-        __syncwarp();
-        double2 *dst = dst_of(g);
-#pragma unroll
-        for (int q = 0; q < 32; q++) {
-            const int p = lane + 32 * q;
-            if (p < N) dst[p] = buf[o33(p)];
-        }
-        __syncwarp();
-        // the buffer is free again: bring in the line after next (generic-proxy reads of the
-        // buffer are ordered before the asynchronous copy that overwrites it)
-        if (lane == 0 && g + 2 * stride < total) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_expect_tx(&bar[i & 1], kBytes);
-            tma_bulk_load(buf, src_of(g + 2 * stride), kBytes, &bar[i & 1]);
-        }
+        if (lane == 0 && grp + 2 * stride < groups) fetch(grp + 2 * stride, s);
     }
-    // after an expired wait, give the copies still in flight (this buffer's and the next one's)
-    // a bounded chance to land before the CTA's shared memory is released
+    // after an expired wait, give the copies still in flight a bounded chance to land before the
+    // CTA's shared memory is released
     if (failed >= 0 && lane == 0) {
-        mbar_wait_parity(&bar[i & 1], (i >> 1) & 1);
-        if (failed + stride < total) mbar_wait_parity(&bar[(i + 1) & 1], ((i + 1) >> 1) & 1);
+        mbar_wait_parity(&bar[it & 1], (it >> 1) & 1);
+        if (failed + stride < groups) mbar_wait_parity(&bar[(it + 1) & 1], ((it + 1) >> 1) & 1);
+    }
+}
+
+// ---- columns: line x of plane p is element j at base + p plane + x + (j - 1) ld.  A 4-D tensor
+// map (re/im, x, j, plane) brings C = LPW neighbouring columns, all rows, into a [j][c] tile; the
+// warp's lanes interleave over the C lines (lane = c + LPW l) so that reading the tile is free of
+// bank conflicts, and the outputs go back through the same tile with a tensor store.
+template <int M> struct WColGeom {
+    using G = WGeom<M>;
+    static constexpr int LPW = G::LPW, N = M - 1;
+    static constexpr int BR = N < 256 ? N : 256;              // rows per TMA box
+    static constexpr int NBOX = (N + BR - 1) / BR;
+    // tensor copies need 128-byte aligned shared-memory addresses: tiles and warp areas are
+    // whole multiples of 8 elements (boxes inside a tile follow each other at LPW * 256
+    // elements, also a multiple of 8, whenever there is more than one)
+    static constexpr int TILE = (LPW * BR * NBOX + 7) / 8 * 8;
+    // line exchange areas offset so that the LPW lines of an 8-lane phase fall on distinct banks
+    static constexpr int BUFC = (G::BUF + 7) / 8 * 8 + (LPW > 1 ? 8 / LPW : 0);
+    static constexpr int WPC = G::WPC;
+    static constexpr int WARP_ELEMS = (2 * TILE + LPW * BUFC + 7) / 8 * 8; // two tiles, one exchange area
+    static constexpr int SMEM = 256 + 16 * WARP_ELEMS * WPC;               // + barriers, + base alignment
+    static_assert(NBOX == 1 || (LPW * BR) % 8 == 0, "box offsets must stay 128-byte aligned");
+};
+
+__device__ __forceinline__ void tma_tile_load(void *dst, const CUtensorMap *map, int x, int j, int p, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(
+            smem_u32(dst)),
+        "l"(map), "r"(0), "r"(x), "r"(j), "r"(p), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_tile_store(const CUtensorMap *map, int x, int j, int p, const void *src) {
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(map),
+                 "r"(0), "r"(x), "r"(j), "r"(p), "r"(smem_u32(src))
+                 : "memory");
+}
+
+template <int M>
+__global__ void __launch_bounds__(32 * WCfg<M>::WPC, 3)
+    k_dst1_wc(const __grid_constant__ CUtensorMap in_map, const __grid_constant__ CUtensorMap out_map, long ncols,
+              long nplanes, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
+    using G = WGeom<M>;
+    using CG = WColGeom<M>;
+    constexpr int      TL = G::TL, LPW = G::LPW, KB = G::KB, N = M - 1, K2 = 2 * KB;
+    constexpr int      BR = CG::BR, NBOX = CG::NBOX;
+    constexpr uint32_t kBoxBytes = LPW * BR * 16;
+    extern __shared__ __align__(128) unsigned char dsm_raw[];
+    // 128-byte aligned start of the tiles (the allocation carries 128 bytes of slack for this)
+    unsigned char *dsm = dsm_raw + ((128u - (smem_u32(dsm_raw) & 127u)) & 127u);
+    const int      lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+    const int      c = lane % LPW, l = lane / LPW; // interleaved: lane = c + LPW l
+    uint64_t      *bar = reinterpret_cast<uint64_t *>(dsm) + 2 * wq;
+    double2       *wbase = reinterpret_cast<double2 *>(dsm + 128) + wq * CG::WARP_ELEMS;
+    if ((smem_u32(wbase) & 127u) != 0) { // cannot happen with the layout above; never issue a misaligned copy
+        if (lane == 0) atomicExch(err, 2);
+        return;
+    }
+    double2   *xbuf = wbase + 2 * CG::TILE + c * CG::BUFC; // the line's exchange area
+    const long cgroups = (ncols + LPW - 1) / LPW;
+    const long groups = cgroups * nplanes;
+    const long stride = (long)gridDim.x * G::WPC;
+    const long g0 = (long)blockIdx.x * G::WPC + wq;
+    if (g0 >= groups) return; // whole warp
+
+    auto fetch = [&](long grp, int s) {
+        const int x0 = (int)((grp % cgroups) * LPW), p = (int)(grp / cgroups);
+        mbar_expect_tx(&bar[s], NBOX * kBoxBytes);
+        for (int b = 0; b < NBOX; b++)
+            tma_tile_load(wbase + s * CG::TILE + b * LPW * BR, &in_map, x0, b * BR, p, &bar[s]);
+    };
+    if (lane == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    if (lane == 0) {
+        fetch(g0, 0);
+        if (g0 + stride < groups) fetch(g0 + stride, 1);
+    }
+    WConst<M> K;
+    K.load(l, tw, sn);
+
+    int  it = 0;
+    long failed = -1;
+    for (long grp = g0; grp < groups; grp += stride, it++) {
+        const int s = it & 1;
+        double2  *tile = wbase + s * CG::TILE;
+        const bool live = (grp % cgroups) * LPW + c < ncols;
+        if (!mbar_wait_parity(&bar[s], (it >> 1) & 1)) {
+            if (lane == 0) atomicExch(err, 1);
+            failed = grp;
+            break;
+        }
+        w_transform<M, true>([&](int j) { return tile[(j - 1) * LPW + c]; }, xbuf, l, live, K);
+        // outputs into the tile ([j][c], rows past N untouched), then one tensor store per box
+#pragma unroll
+        for (int q = 0; q < M / TL; q++) {
+            const int p = l + TL * q;
+            if (p < N) tile[p * LPW + c] = xbuf[(K2 + 1) * (p / K2) + p % K2];
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // tile writes before the store reads
+        __syncwarp();
+        if (lane == 0) {
+            const int x0 = (int)((grp % cgroups) * LPW), pl = (int)(grp / cgroups);
+            for (int b = 0; b < NBOX; b++) tma_tile_store(&out_map, x0, b * BR, pl, tile + b * LPW * BR);
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+            // the tile is read by the store before the next load overwrites it
+            if (grp + 2 * stride < groups) {
+                asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+                fetch(grp + 2 * stride, s);
+            }
+        }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); // stores complete before exit
+        if (failed >= 0) {
+            mbar_wait_parity(&bar[it & 1], (it >> 1) & 1);
+            if (failed + stride < groups) mbar_wait_parity(&bar[(it + 1) & 1], ((it + 1) >> 1) & 1);
+        }
     }
 }
 
@@ -713,18 +917,19 @@ template <int M, bool IS, bool OS> static int launch_fft(Ctx *c, const DstArgs &
     return HH_OK;
 }
 
-static int launch_w1024(Ctx *c, const DstArgs &a) {
+template <int M> static int launch_w(Ctx *c, const DstArgs &a) {
+    using G = WGeom<M>;
     const double2 *tw;
     const double  *sn;
-    HH_TRY(tables_for(c, 1024, &tw, &sn));
-    const int shm = 16 * kDstWarps + (int)(sizeof(double2) * kDstWarpBuf * 2 * kDstWarps);
-    HH_CUDA(cudaFuncSetAttribute(k_dst1_w1024, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
-    int dev = 0, sms = 148;
+    HH_TRY(tables_for(c, M, &tw, &sn));
+    HH_CUDA(cudaFuncSetAttribute(k_dst1_w<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
+    int dev = 0, sms = 148, per_sm = 0;
     HH_CUDA(cudaGetDevice(&dev));
     HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const long lines = a.nlines * a.planes;
-    const long ctas = std::min<long>((lines + kDstWarps - 1) / kDstWarps, 3L * sms);
-    k_dst1_w1024<<<(unsigned)ctas, 32 * kDstWarps, shm, c->stream>>>(a.in, a.out, a.nlines, a.planes, a.in_ld, a.out_ld,
+    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dst1_w<M>, 32 * G::WPC, G::SMEM));
+    const long groups = (a.nlines * a.planes + G::LPW - 1) / G::LPW;
+    const long ctas = std::min<long>((groups + G::WPC - 1) / G::WPC, (long)std::max(1, per_sm) * sms);
+    k_dst1_w<M><<<(unsigned)ctas, 32 * G::WPC, G::SMEM, c->stream>>>(a.in, a.out, a.nlines, a.planes, a.in_ld, a.out_ld,
                                                                      a.in_plane, a.out_plane, tw, sn, c->err_word);
     HH_CUDA(cudaGetLastError());
     c->launches++;
@@ -739,7 +944,16 @@ template <bool IS, bool OS> static int launch_dispatch(Ctx *c, int n, const DstA
         set_error("DST rows must be 16-byte aligned");
         return HH_ERR_INVALID;
     }
-    if (n == 1023 && !IS && !OS) return launch_w1024(c, a);
+    if (!IS && !OS) {
+        switch (n + 1) { // contiguous rows: persistent-warp kernels
+        case 64: return launch_w<64>(c, a);
+        case 128: return launch_w<128>(c, a);
+        case 256: return launch_w<256>(c, a);
+        case 512: return launch_w<512>(c, a);
+        case 1024: return launch_w<1024>(c, a);
+        default: break;
+        }
+    }
     switch (n + 1) {
     case 64: return launch_fft<64, IS, OS>(c, a);
     case 128: return launch_fft<128, IS, OS>(c, a);
@@ -777,8 +991,73 @@ int launch_dst_rows(Ctx *c, int n, long rows, const double2 *in, long in_ld, dou
     return launch_dispatch<false, false>(c, n, a);
 }
 
+// 4-D tensor map over (re/im, column x, row j, plane) of complex doubles, boxes of `box_cols`
+// columns by `box_rows` rows.
+static int encode_col_map(CUtensorMap *map, const double2 *base, long ncols, long rows, long planes, long ld,
+                          long plane_stride, int box_cols, int box_rows) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        cudaDriverEntryPointQueryResult q;
+        void                           *fn = nullptr;
+        HH_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (!fn || q != cudaDriverEntryPointSuccess) {
+            set_error("cuTensorMapEncodeTiled is not available");
+            return HH_ERR_CUDA;
+        }
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[4] = {2, (cuuint64_t)ncols, (cuuint64_t)rows, (cuuint64_t)planes};
+    const cuuint64_t strides[3] = {16, (cuuint64_t)ld * 16, (cuuint64_t)plane_stride * 16};
+    const cuuint32_t box[4] = {2, (cuuint32_t)box_cols, (cuuint32_t)box_rows, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult   r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double2 *>(base), dims, strides, box,
+                                estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return HH_ERR_CUDA;
+    }
+    return HH_OK;
+}
+
+template <int M>
+static int launch_wc(Ctx *c, long ncols, long planes, const double2 *in, long ld, long plane_stride, double2 *out) {
+    using G = WGeom<M>;
+    using CG = WColGeom<M>;
+    const double2 *tw;
+    const double  *sn;
+    HH_TRY(tables_for(c, M, &tw, &sn));
+    CUtensorMap in_map, out_map;
+    HH_TRY(encode_col_map(&in_map, in, ncols, M - 1, planes, ld, plane_stride, G::LPW, CG::BR));
+    HH_TRY(encode_col_map(&out_map, out, ncols, M - 1, planes, ld, plane_stride, G::LPW, CG::BR));
+    HH_CUDA(cudaFuncSetAttribute(k_dst1_wc<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, CG::SMEM));
+    int dev = 0, sms = 148, per_sm = 0;
+    HH_CUDA(cudaGetDevice(&dev));
+    HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dst1_wc<M>, 32 * G::WPC, CG::SMEM));
+    const long groups = (ncols + G::LPW - 1) / G::LPW * planes;
+    const long ctas = std::min<long>((groups + G::WPC - 1) / G::WPC, (long)std::max(1, per_sm) * sms);
+    k_dst1_wc<M><<<(unsigned)ctas, 32 * G::WPC, CG::SMEM, c->stream>>>(in_map, out_map, ncols, planes, tw, sn,
+                                                                       c->err_word);
+    HH_CUDA(cudaGetLastError());
+    c->launches++;
+    return HH_OK;
+}
+
 int launch_dst_cols(Ctx *c, int n, long ncols, long planes, const double2 *in, long ld, long plane_stride,
                     double2 *out) {
+    // tensor maps need 16-byte aligned bases (always true for double2) and byte strides below 2^40
+    // (the tensor-map box never exceeds the tensor: at least LPW columns)
+    if (planes > 0 && ld * 16 < (1L << 40) && plane_stride * 16 < (1L << 40) && planes < (1L << 31)) {
+        switch (n + 1) {
+        case 64: if (ncols >= WGeom<64>::LPW) return launch_wc<64>(c, ncols, planes, in, ld, plane_stride, out); break;
+        case 128: if (ncols >= WGeom<128>::LPW) return launch_wc<128>(c, ncols, planes, in, ld, plane_stride, out); break;
+        case 256: if (ncols >= WGeom<256>::LPW) return launch_wc<256>(c, ncols, planes, in, ld, plane_stride, out); break;
+        case 512: if (ncols >= WGeom<512>::LPW) return launch_wc<512>(c, ncols, planes, in, ld, plane_stride, out); break;
+        case 1024: if (ncols >= WGeom<1024>::LPW) return launch_wc<1024>(c, ncols, planes, in, ld, plane_stride, out); break;
+        default: break;
+        }
+    }
     DstArgs a{in, out, ncols, planes, ld, ld, plane_stride, plane_stride};
     return launch_dispatch<true, true>(c, n, a);
 }

@@ -67,7 +67,8 @@ def test_dst_rows_pitched(ctx, oracle, n):
     assert np.all(o[:, n:] == 7.0 + 7.0j)  # nothing written past the line
 
 
-@pytest.mark.parametrize("n,ncols,planes", [(255, 255, 3), (63, 100, 2), (100, 37, 2), (1023, 64, 1), (7, 5, 4)])
+@pytest.mark.parametrize("n,ncols,planes", [(255, 255, 3), (63, 100, 2), (100, 37, 2), (1023, 64, 1), (7, 5, 4),
+                                              (127, 33, 3), (511, 7, 2), (255, 1, 5), (63, 3, 7)])
 def test_dst_cols_matches_oracle(ctx, oracle, n, ncols, planes):
     rng = np.random.default_rng(n + ncols)
     x = rng.standard_normal((planes, n, ncols)) + 1j * rng.standard_normal((planes, n, ncols))
@@ -100,3 +101,25 @@ def test_dst2_planes_matches_reference_plane_transform(ctx, oracle, nx, ny):
             else:
                 ref[p] += 1j * out
     assert rel_err(_host(t), ref) < 1e-13
+
+
+@pytest.mark.parametrize("n", [63, 255, 1023])
+def test_dst_cols_pitched(ctx, oracle, n):
+    """Columns inside pitched planes (ld > ncols, plane stride > n*ld), written in place; values
+    outside the columns stay untouched."""
+    ncols, ld, planes = 9, 13, 3
+    pstride = n * ld + 5
+    rng = np.random.default_rng(n)
+    buf = rng.standard_normal(planes * pstride) + 1j * rng.standard_normal(planes * pstride)
+    t = _dev(buf)
+    ctx.dst1_cols(n, ncols, planes, t, ld, pstride, t)
+    ctx.synchronize()
+    o = _host(t)
+    for p in range(planes):
+        blk = buf[p * pstride: p * pstride + n * ld].reshape(n, ld)
+        got = o[p * pstride: p * pstride + n * ld].reshape(n, ld)
+        want = oracle.dst1_rows(np.ascontiguousarray(blk[:, :ncols].T)).T
+        assert rel_err(got[:, :ncols], want) < 1e-13
+        assert np.array_equal(got[:, ncols:], blk[:, ncols:])
+    for p in range(planes - 1):
+        assert np.array_equal(o[p * pstride + n * ld:(p + 1) * pstride], buf[p * pstride + n * ld:(p + 1) * pstride])
