@@ -184,6 +184,56 @@ def run_reference(args, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def secondary_configs(hh, ctx, st, torch) -> dict:
+    """Device-resident solves/s of the other plain-FP64 configurations named with the metric:
+    3D N=255 order 6 k=30 batch 4 (16 sine modes, p,q,r <= 64) and 2D N=2047 order 6 batch 16,
+    k in {10, 100, 400} (8 modes, p,q <= 20).  Short CUDA-event timings of captured graphs."""
+    from hackathon_b200 import workload as W
+    out = {}
+    cases = [("3d_n255_o6_k30_b4", 3, 255, 6, [30.0], 4), ("2d_n2047_o6_b16", 2, 2047, 6, [10.0, 100.0, 400.0], 16)]
+    for name, dim, n, order, ks, batch in cases:
+        if dim == 3:
+            f_host = np.stack([W.source_3d(n, W.sine_modes(2000 + b, 16, 64, dim=3))[1:-1, 1:-1, 1:-1]
+                               for b in range(batch)])
+        else:
+            f_host = np.stack([W.source_2d(n, W.sine_modes(3000 + b, 8, 20), fast=True)[1:-1, 1:-1]
+                               for b in range(batch)])
+        f = torch.from_numpy(np.ascontiguousarray(f_host)).cuda()
+        u = torch.empty_like(f)
+        plans = [hh.Plan.helmholtz(ctx, dim, n, order, k) for k in ks]
+        graphs = []
+        for p in plans:
+            p.tune(batch)
+            for _ in range(3):
+                p.solve_source(f, u, batch)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=st):
+                p.solve_source(f, u, batch)
+            graphs.append(g)
+        for g in graphs:
+            g.replay()
+        torch.cuda.synchronize()
+        steps = 30
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for s in range(steps):
+            graphs[s % len(graphs)].replay()
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        pts = batch * n ** dim
+        out[name] = {"solves_per_s": batch / (ms / 1000.0), "ms_per_step": ms,
+                     "gpoints_per_s": pts / (ms / 1000.0) / 1e9,
+                     "hbm_frac_of_96B_per_point": 96.0 * pts / (ms / 1000.0) / 1e9 / measured_hbm_peak()[0],
+                     "line_solve_variants": [p.variant for p in plans]}
+        del graphs
+        for p in plans:
+            p.close()
+        del f, u
+        torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -192,6 +242,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the 3D 255^3 and 2D 2047^2 figures")
     ap.add_argument("--batch", type=int, default=BATCH, help="right-hand sides per step (profiling runs)")
     ap.add_argument("--variant", type=int, default=None,
                     help="force one line-solve kernel variant instead of hh_plan_tune (profiling runs)")
@@ -338,6 +389,8 @@ def main():
             "timing": "CUDA events on the launch stream around CUDA-graph replays (one graph per (order, k))",
             "clocks": clk.summary(),
         }
+        if world == 1 and not args.no_secondary:
+            line["secondary"] = secondary_configs(hh, ctx, st, torch)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
