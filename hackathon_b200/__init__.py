@@ -25,6 +25,20 @@ STATUS = {0: "HH_OK", 1: "HH_ERR_INVALID", 2: "HH_ERR_CUDA", 3: "HH_ERR_NOMEM", 
 # every symbol include/hh.h declares, with its ctypes signature
 _vp, _i, _l, _d, _sz = C.c_void_p, C.c_int, C.c_long, C.c_double, C.c_size_t
 _dp = C.POINTER(C.c_double)
+
+
+class Request(C.Structure):
+    """include/hh.h hh_request"""
+    _fields_ = [("dim", C.c_int), ("n", C.c_int), ("order", C.c_int), ("k_re", C.c_double), ("k_im", C.c_double),
+                ("nrhs", C.c_int), ("on_device", C.c_int), ("f", C.c_void_p), ("u", C.c_void_p)]
+
+
+class RequestInfo(C.Structure):
+    """include/hh.h hh_request_info"""
+    _fields_ = [("status", C.c_int), ("t_submit", C.c_double), ("t_start", C.c_double), ("t_done", C.c_double),
+                ("batch_rhs", C.c_int)]
+
+
 SIGNATURES = {
     "hh_last_error": (C.c_char_p, []),
     "hh_version": (_i, []),
@@ -57,6 +71,12 @@ SIGNATURES = {
     "hh_coefficients3d": (_i, [_i, _i, _d, _d, C.POINTER(_vp)]),
     "hh_ctx_set_stage_timing": (_i, [_vp, _i]),
     "hh_ctx_stage_times": (_i, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
+    "hh_server_create": (_i, [_i, _sz, _i, C.POINTER(_vp)]),
+    "hh_server_submit": (_i, [_vp, C.POINTER(Request), C.POINTER(C.c_longlong)]),
+    "hh_server_wait": (_i, [_vp, C.c_longlong, C.POINTER(RequestInfo)]),
+    "hh_server_stats": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(_sz), C.POINTER(_i)]),
+    "hh_server_clock": (_d, [_vp]),
+    "hh_server_destroy": (_i, [_vp]),
 }
 
 _lib = None
@@ -249,3 +269,50 @@ def coefficients(dim: int, n: int, order: int, k: complex) -> dict:
     f = lib().hh_coefficients2d if dim == 2 else lib().hh_coefficients3d
     check(f(n, order, k.real, k.imag, ptrs), "hh_coefficients")
     return dict(zip(names, arrs))
+
+
+class Server:
+    """Request loop over one device (include/hh.h hh_server_*): submit returns at once, wait
+    blocks for one request.  Buffers (numpy arrays, torch tensors or raw addresses) must stay
+    alive until the request's wait returns."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 150 << 30, streams: int = 4):
+        self.h = _vp()
+        check(lib().hh_server_create(device, hbm_budget, streams, C.byref(self.h)), "hh_server_create")
+        self._keep = {}
+
+    def submit(self, dim: int, n: int, order: int, k: complex, nrhs: int, f, u, on_device: bool = False) -> int:
+        k = complex(k)
+        r = Request(dim, n, order, k.real, k.imag, nrhs, int(on_device), _addr(f), _addr(u))
+        rid = C.c_longlong()
+        check(lib().hh_server_submit(self.h, C.byref(r), C.byref(rid)), "hh_server_submit")
+        self._keep[rid.value] = (f, u)
+        return rid.value
+
+    def wait(self, rid: int) -> dict:
+        info = RequestInfo()
+        rc = lib().hh_server_wait(self.h, rid, C.byref(info))
+        self._keep.pop(rid, None)
+        check(rc, "hh_server_wait")
+        return {"t_submit": info.t_submit, "t_start": info.t_start, "t_done": info.t_done,
+                "batch_rhs": info.batch_rhs}
+
+    def stats(self) -> dict:
+        done, used, plans = C.c_longlong(), C.c_size_t(), C.c_int()
+        check(lib().hh_server_stats(self.h, C.byref(done), C.byref(used), C.byref(plans)), "hh_server_stats")
+        return {"completed": done.value, "bytes_in_use": used.value, "plans": plans.value}
+
+    def clock(self) -> float:
+        return float(lib().hh_server_clock(self.h))
+
+    def close(self):
+        if self.h:
+            lib().hh_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

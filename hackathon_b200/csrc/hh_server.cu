@@ -1,0 +1,430 @@
+// Request loop over one device (include/hh.h, "serving").
+//
+// The reference has no serving layer: its Direct_Solver solves one problem per process.  This
+// loop keeps the solver's per-problem set-up resident and streams requests through it:
+//  * one plan per (dim, n, order, k) stays on the device (twiddles and sine tables are shared by
+//    the context, factors and Pade tables belong to the plan) and is evicted least recently used
+//    when the HBM budget needs the room;
+//  * continuous batching: when the dispatcher picks a request it also takes every queued request
+//    of the same plan (small ones, up to kMergeRhs right-hand sides in all) and runs them as one
+//    batched solve;
+//  * admission: a batch starts only while plans plus in-flight staging stay within the budget;
+//    otherwise it waits for running batches to finish;
+//  * batches go round-robin to several CUDA streams, so work of different requests overlaps on
+//    the device; completion is signalled by a host function enqueued behind each batch.
+// Every batched solve computes each right-hand side with exactly the arithmetic of a solo solve
+// on the same plan (the kernels never mix right-hand sides), so results are bitwise identical.
+#include "hh_internal.cuh"
+
+#include <hh.h>
+
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <tuple>
+#include <vector>
+
+namespace {
+
+constexpr int  kMergeRhs = 64;          // right-hand sides in one merged batch at most
+constexpr long kMergePoints = 1L << 22; // requests with more points than this run on their own
+
+using Key = std::tuple<int, int, int, double, double>; // dim, n, order, k_re, k_im
+
+struct Req {
+    long long       id = 0;
+    hh_request      r{};
+    hh_request_info info{};
+    bool            done = false;
+    std::string     err;
+};
+
+struct PlanEntry {
+    hh_plan *plan = nullptr;
+    size_t   bytes = 0;
+    int      inflight = 0;
+    long     last_use = 0;
+};
+
+struct Batch;
+
+} // namespace
+
+struct hh_server {
+    int                                 device = 0;
+    hh_ctx                             *ctx = nullptr;
+    std::vector<cudaStream_t>           streams;
+    cudaMemPool_t                       pool = nullptr;
+    int                                *flags = nullptr; // pinned, one slot per stream
+    size_t                              budget = 0, used = 0;
+    std::mutex                          m;
+    std::condition_variable             cv;
+    std::deque<Req *>                   queue;
+    std::map<long long, Req *>          reqs;
+    std::map<Key, PlanEntry>            plans;
+    long long                           next_id = 1, completed = 0;
+    long                                tick = 0;
+    int                                 inflight = 0, rr = 0;
+    bool                                stop = false;
+    std::thread                         worker;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    double now() const {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+namespace {
+
+struct Batch {
+    hh_server         *s = nullptr;
+    std::vector<Req *> reqs;
+    Key                key;
+    size_t             staging = 0;
+    bool               reserved = false; // staging counted in s->used
+    bool               plan_ref = false; // holds an in-flight reference on its plan
+    int               *flag = nullptr;   // pinned copy of the device error word after the batch
+};
+
+long points_of(const hh_request &r) {
+    long p = 1;
+    for (int d = 0; d < r.dim; d++) p *= r.n;
+    return p;
+}
+
+size_t plan_bytes(const hh_request &r) {
+    // segment pivots (2 per 16 points), row tables, multipliers: a conservative estimate
+    return (size_t)(2 * points_of(r)) * 16 + (size_t)r.n * 4096 + (1 << 20);
+}
+
+// completion: runs on a CUDA host-function thread after the batch's last operation (no CUDA calls)
+void batch_done(void *arg) {
+    Batch     *b = static_cast<Batch *>(arg);
+    hh_server *s = b->s;
+    {
+        std::lock_guard<std::mutex> g(s->m);
+        const double t = s->now();
+        const bool   bad = b->flag && *b->flag != 0; // a kernel of this context hit a bounded wait
+        for (Req *q : b->reqs) {
+            q->done = true;
+            q->info.t_done = t;
+            q->info.status = bad ? HH_ERR_DEVICE : HH_OK;
+            if (bad) q->err = "a kernel reported an expired bounded wait";
+        }
+        s->used -= b->staging;
+        s->inflight--;
+        s->completed += (long long)b->reqs.size();
+        auto it = s->plans.find(b->key);
+        if (it != s->plans.end()) it->second.inflight--;
+    }
+    s->cv.notify_all();
+    delete b;
+}
+
+// the batch could not run: release what it holds and complete its requests with `rc` (lock not held)
+void fail_batch(hh_server *s, Batch *b, int rc, const std::string &msg) {
+    {
+        std::lock_guard<std::mutex> g(s->m);
+        const double t = s->now();
+        for (Req *q : b->reqs) {
+            q->done = true;
+            q->info.t_done = t;
+            q->info.status = rc;
+            q->err = msg;
+        }
+        if (b->reserved) s->used -= b->staging;
+        s->inflight--;
+        if (b->plan_ref) {
+            auto it = s->plans.find(b->key);
+            if (it != s->plans.end()) it->second.inflight--;
+        }
+    }
+    s->cv.notify_all();
+    delete b;
+}
+
+// idle plans to evict, least recently used first, until `need` more bytes fit; they leave the map
+// and the budget here and are destroyed by the caller without the lock (destroying a plan
+// synchronizes the device, which waits for completion callbacks that take the lock)
+std::vector<hh_plan *> pick_victims(hh_server *s, size_t need) {
+    std::vector<hh_plan *> out;
+    while (s->used + need > s->budget) {
+        auto victim = s->plans.end();
+        for (auto it = s->plans.begin(); it != s->plans.end(); ++it)
+            if (it->second.inflight == 0 && (victim == s->plans.end() || it->second.last_use < victim->second.last_use))
+                victim = it;
+        if (victim == s->plans.end()) break;
+        out.push_back(victim->second.plan);
+        s->used -= victim->second.bytes;
+        s->plans.erase(victim);
+    }
+    return out;
+}
+
+// Enqueue the batch on the next stream.  On failure nothing of it is left in flight.
+int run_batch(hh_server *s, Batch *b, hh_plan *plan) {
+    const hh_request &r0 = b->reqs[0]->r;
+    const long        field = points_of(r0);
+    const int         si = s->rr++ % (int)s->streams.size();
+    cudaStream_t      st = s->streams[(size_t)si];
+    double2          *buf = nullptr;
+    auto enqueue = [&]() -> int {
+        HH_TRY(hh_ctx_set_stream(s->ctx, st));
+        int total = 0;
+        for (Req *q : b->reqs) total += q->r.nrhs;
+        if (b->staging == 0) {
+            HH_TRY(hh_solve_source(plan, r0.f, r0.u, total)); // straight from the caller's device buffers
+        } else {
+            HH_CUDA(cudaMallocFromPoolAsync((void **)&buf, b->staging, s->pool, st));
+            long off = 0;
+            for (Req *q : b->reqs) {
+                const size_t bytes = sizeof(double2) * (size_t)field * q->r.nrhs;
+                HH_CUDA(cudaMemcpyAsync(buf + off, q->r.f, bytes,
+                                        q->r.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+                off += field * q->r.nrhs;
+            }
+            HH_TRY(hh_solve_source(plan, (const double *)buf, (double *)buf, total));
+            off = 0;
+            for (Req *q : b->reqs) {
+                const size_t bytes = sizeof(double2) * (size_t)field * q->r.nrhs;
+                HH_CUDA(cudaMemcpyAsync(q->r.u, buf + off, bytes,
+                                        q->r.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+                off += field * q->r.nrhs;
+            }
+            HH_CUDA(cudaFreeAsync(buf, st));
+            buf = nullptr;
+        }
+        b->flag = s->flags + si;
+        HH_CUDA(cudaMemcpyAsync(b->flag, reinterpret_cast<hh::Ctx *>(s->ctx)->err_word, sizeof(int),
+                                cudaMemcpyDeviceToHost, st));
+        HH_CUDA(cudaLaunchHostFunc(st, batch_done, b));
+        return HH_OK;
+    };
+    const int rc = enqueue();
+    if (rc != HH_OK) {
+        cudaStreamSynchronize(st); // copies already queued must not outlive the request
+        if (buf) cudaFree(buf);
+    }
+    return rc;
+}
+
+void dispatcher(hh_server *s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->m);
+    for (;;) {
+        s->cv.wait(lk, [&] { return s->stop || !s->queue.empty(); });
+        if (s->queue.empty()) {
+            if (s->stop) break;
+            continue;
+        }
+        // the head request and every queued small request of the same plan (continuous batching)
+        Req       *head = s->queue.front();
+        const Key  key{head->r.dim, head->r.n, head->r.order, head->r.k_re, head->r.k_im};
+        const long field = points_of(head->r);
+        Batch     *b = new Batch;
+        b->s = s;
+        b->key = key;
+        b->reqs.push_back(head);
+        int rhs = head->r.nrhs;
+        if (field * head->r.nrhs <= kMergePoints) {
+            for (Req *q : s->queue) {
+                if (q == head || rhs >= kMergeRhs) continue;
+                const Key kq{q->r.dim, q->r.n, q->r.order, q->r.k_re, q->r.k_im};
+                if (kq == key && field * q->r.nrhs <= kMergePoints && rhs + q->r.nrhs <= kMergeRhs) {
+                    b->reqs.push_back(q);
+                    rhs += q->r.nrhs;
+                }
+            }
+        }
+        const bool direct = b->reqs.size() == 1 && head->r.on_device;
+        b->staging = direct ? 0 : sizeof(double2) * (size_t)field * rhs;
+        auto need = [&]() { return b->staging + (s->plans.count(key) ? 0 : plan_bytes(head->r)); };
+        // admission by HBM budget: wait for running batches, then evict idle plans
+        while (s->used + need() > s->budget && s->inflight > 0) s->cv.wait(lk);
+        std::vector<hh_plan *> victims = pick_victims(s, need());
+        if (!victims.empty()) {
+            lk.unlock();
+            for (hh_plan *v : victims) hh_plan_destroy(v);
+            lk.lock();
+        }
+        for (Req *q : b->reqs) s->queue.erase(std::find(s->queue.begin(), s->queue.end(), q));
+        const double t = s->now();
+        for (Req *q : b->reqs) {
+            q->info.t_start = t;
+            q->info.batch_rhs = rhs;
+        }
+        s->inflight++;
+        const bool   create = s->plans.count(key) == 0;
+        const size_t pbytes = create ? plan_bytes(head->r) : 0;
+        if (s->used + b->staging + pbytes > s->budget) {
+            lk.unlock();
+            fail_batch(s, b, HH_ERR_NOMEM, "request does not fit in the server's HBM budget");
+            lk.lock();
+            continue;
+        }
+        s->used += b->staging + pbytes; // staging and (reserved) plan memory
+        b->reserved = true;
+        hh_plan *plan = nullptr;
+        if (create) {
+            lk.unlock(); // plan set-up synchronizes its stream
+            const hh_request &r = head->r;
+            const int rc = r.dim == 2 ? hh_plan2d_create_helmholtz(s->ctx, r.n, r.order, r.k_re, r.k_im, &plan)
+                                      : hh_plan3d_create_helmholtz(s->ctx, r.n, r.order, r.k_re, r.k_im, &plan);
+            const std::string msg = rc == HH_OK ? std::string() : std::string(hh_last_error());
+            lk.lock();
+            if (rc != HH_OK) {
+                s->used -= pbytes;
+                lk.unlock();
+                fail_batch(s, b, rc, msg);
+                lk.lock();
+                continue;
+            }
+            PlanEntry e;
+            e.plan = plan;
+            e.bytes = pbytes;
+            s->plans.emplace(key, e);
+        }
+        PlanEntry &pe = s->plans[key];
+        pe.inflight++;
+        pe.last_use = ++s->tick;
+        plan = pe.plan;
+        b->plan_ref = true;
+        lk.unlock();
+        const int rc = run_batch(s, b, plan);
+        if (rc != HH_OK) fail_batch(s, b, rc, hh_last_error());
+        lk.lock();
+    }
+}
+
+bool valid(const hh_request *r) {
+    return r && (r->dim == 2 || r->dim == 3) && r->n >= 1 && (r->order == 2 || r->order == 4 || r->order == 6) &&
+           r->nrhs >= 1 && r->nrhs <= 65535 && r->f && r->u;
+}
+
+} // namespace
+
+using hh::set_error;
+
+extern "C" int hh_server_create(int device, size_t budget, int streams, hh_server **out) {
+    if (!out || streams < 1 || streams > 64 || budget == 0) {
+        set_error("hh_server_create: invalid arguments");
+        return HH_ERR_INVALID;
+    }
+    *out = nullptr;
+    hh_server *s = new hh_server;
+    s->device = device;
+    s->budget = budget;
+    int rc = hh_ctx_create(device, nullptr, &s->ctx);
+    if (rc != HH_OK) { delete s; return rc; }
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaError_t e = cudaMemPoolCreate(&s->pool, &props);
+    if (e == cudaSuccess) {
+        unsigned long long keep = (unsigned long long)budget; // keep freed staging in the pool up to the budget
+        e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    if (e == cudaSuccess) e = cudaHostAlloc((void **)&s->flags, sizeof(int) * 64, cudaHostAllocDefault);
+    if (e == cudaSuccess) memset(s->flags, 0, sizeof(int) * 64);
+    for (int i = 0; i < streams && e == cudaSuccess; i++) {
+        cudaStream_t st;
+        e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        if (e == cudaSuccess) s->streams.push_back(st);
+    }
+    if (e != cudaSuccess) {
+        set_error("hh_server_create: %s", cudaGetErrorString(e));
+        for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
+        if (s->pool) cudaMemPoolDestroy(s->pool);
+        if (s->flags) cudaFreeHost(s->flags);
+        hh_ctx_destroy(s->ctx);
+        delete s;
+        return HH_ERR_CUDA;
+    }
+    s->worker = std::thread(dispatcher, s);
+    *out = s;
+    return HH_OK;
+}
+
+extern "C" int hh_server_submit(hh_server *s, const hh_request *r, long long *id) {
+    if (!s || !valid(r) || !id) {
+        set_error("hh_server_submit: invalid request");
+        return HH_ERR_INVALID;
+    }
+    Req *q = new Req;
+    q->r = *r;
+    {
+        std::lock_guard<std::mutex> g(s->m);
+        if (s->stop) {
+            delete q;
+            set_error("hh_server_submit: server is shutting down");
+            return HH_ERR_INVALID;
+        }
+        q->id = s->next_id++;
+        q->info.t_submit = s->now();
+        s->reqs[q->id] = q;
+        s->queue.push_back(q);
+        *id = q->id;
+    }
+    s->cv.notify_all();
+    return HH_OK;
+}
+
+extern "C" int hh_server_wait(hh_server *s, long long id, hh_request_info *info) {
+    if (!s) return HH_ERR_INVALID;
+    std::unique_lock<std::mutex> lk(s->m);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) {
+        set_error("hh_server_wait: unknown request %lld", id);
+        return HH_ERR_INVALID;
+    }
+    Req *q = it->second;
+    s->cv.wait(lk, [&] { return q->done; });
+    if (info) *info = q->info;
+    const int rc = q->info.status;
+    if (rc != HH_OK) set_error("%s", q->err.c_str());
+    s->reqs.erase(it);
+    delete q;
+    return rc;
+}
+
+extern "C" int hh_server_stats(hh_server *s, long long *done, size_t *bytes_in_use, int *plans) {
+    if (!s) return HH_ERR_INVALID;
+    std::lock_guard<std::mutex> g(s->m);
+    if (done) *done = s->completed;
+    if (bytes_in_use) *bytes_in_use = s->used;
+    if (plans) *plans = (int)s->plans.size();
+    return HH_OK;
+}
+
+extern "C" double hh_server_clock(hh_server *s) { return s ? s->now() : 0.0; }
+
+extern "C" int hh_server_destroy(hh_server *s) {
+    if (!s) return HH_OK;
+    {
+        std::lock_guard<std::mutex> g(s->m);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    // let every batch finish (their host functions touch the server)
+    for (cudaStream_t st : s->streams) cudaStreamSynchronize(st);
+    {
+        std::unique_lock<std::mutex> lk(s->m);
+        s->cv.wait(lk, [&] { return s->inflight == 0; });
+    }
+    for (auto &kv : s->plans) hh_plan_destroy(kv.second.plan);
+    for (auto &kv : s->reqs) delete kv.second;
+    hh_ctx_destroy(s->ctx); // while its current stream (one of the server's) still exists
+    for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
+    cudaMemPoolDestroy(s->pool);
+    cudaFreeHost(s->flags);
+    delete s;
+    return HH_OK;
+}

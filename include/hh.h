@@ -130,6 +130,41 @@ int hh_solve_source_host(hh_plan *plan, const double *f_host, double *u_host, in
 int hh_coefficients2d(int n, int order, double k_re, double k_im, double *const out[6]);
 int hh_coefficients3d(int n, int order, double k_re, double k_im, double *const out[12]);
 
+/* ---------------------------------------------------------------- serving ---- */
+/* A request loop over one device (no counterpart in the reference, whose Direct_Solver solves
+ * one problem per process).  hh_server_submit queues a request and returns at once; a
+ * dispatcher thread solves it asynchronously:
+ *  - one plan per (dim, n, order, k) stays resident (least recently used plans are evicted
+ *    when the HBM budget needs the room);
+ *  - continuous batching: queued requests of the same plan (up to 64 right-hand sides, each
+ *    request at most 4M points) run as one batched solve;
+ *  - admission: a batch starts while plans plus in-flight staging fit the HBM budget, otherwise
+ *    it waits for running batches; a request that can never fit fails with HH_ERR_NOMEM;
+ *  - batches go round-robin to `streams` CUDA streams, so requests overlap on the device.
+ * Each result is bitwise the result of hh_solve_source on a plan of the same problem.  Host
+ * buffers should be pinned for copies to overlap; device buffers (on_device = 1) are used
+ * directly when a request runs alone.  Buffers must stay valid until hh_server_wait returns. */
+typedef struct hh_server hh_server;
+typedef struct {
+    int           dim, n, order; /* 2 or 3; interior points per direction; 2, 4 or 6 */
+    double        k_re, k_im;    /* constant wavenumber                               */
+    int           nrhs;          /* right-hand sides (1..65535)                       */
+    int           on_device;     /* 0: f and u are host memory, 1: device memory      */
+    const double *f;             /* nrhs * n^dim complex source samples (interior)    */
+    double       *u;             /* nrhs * n^dim complex solution                     */
+} hh_request;
+typedef struct {
+    int    status;                  /* HH_OK or the failure code                      */
+    double t_submit, t_start, t_done; /* seconds on hh_server_clock                   */
+    int    batch_rhs;               /* right-hand sides of the batch it ran in        */
+} hh_request_info;
+int    hh_server_create(int device, size_t hbm_budget_bytes, int streams, hh_server **out);
+int    hh_server_submit(hh_server *s, const hh_request *r, long long *id);
+int    hh_server_wait(hh_server *s, long long id, hh_request_info *info); /* blocks; frees the id */
+int    hh_server_stats(hh_server *s, long long *completed, size_t *bytes_in_use, int *plans);
+double hh_server_clock(hh_server *s);
+int    hh_server_destroy(hh_server *s); /* finishes every submitted request first */
+
 #ifdef __cplusplus
 }
 #endif
