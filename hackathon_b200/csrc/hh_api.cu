@@ -53,6 +53,19 @@ static int upload(Ctx *c, void *dst, const void *src, size_t bytes) {
     return HH_OK;
 }
 
+// Plan memory: from the context's pool in stream order when it has one (the request loop's
+// contexts: no device-wide synchronization on allocation or release), else cudaMalloc/cudaFree.
+static int dalloc(Ctx *c, void **p, size_t bytes) {
+    if (c->pool) HH_CUDA(cudaMallocFromPoolAsync(p, bytes, c->pool, c->stream));
+    else HH_CUDA(cudaMalloc(p, bytes));
+    return HH_OK;
+}
+static void dfree(Ctx *c, void *p) {
+    if (!p) return;
+    if (c->pool) cudaFreeAsync(p, c->stream);
+    else cudaFree(p);
+}
+
 } // namespace hh
 
 using namespace hh;
@@ -247,12 +260,13 @@ extern "C" int hh_dst2_planes(hh_ctx *x, int nx, int ny, long nplanes, const dou
 static int plan_alloc(hh_plan *pl) {
     Plan &p = pl->p;
     p.ctx->plans.push_back(&p);
-    HH_CUDA(cudaMalloc(&p.Pv, sizeof(double2) * (size_t)segment_count(p.rows) * p.lines));
+    Ctx *c = p.ctx;
+    HH_TRY(dalloc(c, (void **)&p.Pv, sizeof(double2) * (size_t)segment_count(p.rows) * p.lines));
     p.prow = padded_rows(p.rows);
-    HH_CUDA(cudaMalloc(&p.rowc, sizeof(double2) * 4 * (size_t)p.prow));
-    HH_CUDA(cudaMalloc(&p.subt, sizeof(double2) * 4 * (size_t)p.prow));
-    HH_CUDA(cudaMalloc(&p.diagt, sizeof(double2) * 4 * (size_t)p.prow));
-    HH_CUDA(cudaMalloc(&p.mu, sizeof(double) * 3 * (size_t)p.lines));
+    HH_TRY(dalloc(c, (void **)&p.rowc, sizeof(double2) * 4 * (size_t)p.prow));
+    HH_TRY(dalloc(c, (void **)&p.subt, sizeof(double2) * 4 * (size_t)p.prow));
+    HH_TRY(dalloc(c, (void **)&p.diagt, sizeof(double2) * 4 * (size_t)p.prow));
+    HH_TRY(dalloc(c, (void **)&p.mu, sizeof(double) * 3 * (size_t)p.lines));
     return HH_OK;
 }
 
@@ -263,13 +277,14 @@ static void plan_free(hh_plan *pl) {
         for (size_t i = 0; i < v.size(); i++)
             if (v[i] == &p) { v.erase(v.begin() + (long)i); break; }
     }
-    cudaFree(p.Pv);
-    cudaFree(p.rowc);
-    cudaFree(p.subt);
-    cudaFree(p.diagt);
-    cudaFree(p.mu);
-    cudaFree(p.pade_l);
-    cudaFree(p.pade_u);
+    Ctx *c = p.ctx;
+    dfree(c, p.Pv);
+    dfree(c, p.rowc);
+    dfree(c, p.subt);
+    dfree(c, p.diagt);
+    dfree(c, p.mu);
+    dfree(c, p.pade_l);
+    dfree(c, p.pade_u);
 }
 
 // [1 10 1] Pade factors along the line direction (the reference's constant-coefficient solves,
@@ -303,10 +318,10 @@ static int plan_pade(hh_plan *pl) {
                 return HH_ERR_UNSUPPORTED;
             }
     }
-    HH_CUDA(cudaMalloc(&p.pade_l, sizeof(double) * (size_t)p.prow));
-    HH_CUDA(cudaMalloc(&p.pade_u, sizeof(double) * (size_t)p.prow));
-    HH_CUDA(cudaMemcpy(p.pade_l, L.data(), sizeof(double) * (size_t)p.prow, cudaMemcpyHostToDevice));
-    HH_CUDA(cudaMemcpy(p.pade_u, Ui.data(), sizeof(double) * (size_t)p.prow, cudaMemcpyHostToDevice));
+    HH_TRY(dalloc(p.ctx, (void **)&p.pade_l, sizeof(double) * (size_t)p.prow));
+    HH_TRY(dalloc(p.ctx, (void **)&p.pade_u, sizeof(double) * (size_t)p.prow));
+    HH_TRY(upload(p.ctx, p.pade_l, L.data(), sizeof(double) * (size_t)p.prow));
+    HH_TRY(upload(p.ctx, p.pade_u, Ui.data(), sizeof(double) * (size_t)p.prow));
     return HH_OK;
 }
 
@@ -358,7 +373,9 @@ static int plan_factor(hh_plan *pl, const std::vector<double2> &sub, const std::
     if (rc == HH_OK) rc = upload(c, p.rowc, psup.data(), tb);
     if (rc == HH_OK) rc = upload(c, p.mu, mu.data(), sizeof(double) * 3 * (size_t)p.lines);
     if (rc == HH_OK) rc = launch_factor(&p, p.subt, p.diagt, p.rowc);
-    cudaError_t e = cudaStreamSynchronize(c->stream);
+    // contexts with a pool (the request loop) keep set-up asynchronous: its failures surface at
+    // the next synchronization of the stream
+    cudaError_t e = c->pool ? cudaGetLastError() : cudaStreamSynchronize(c->stream);
     if (rc != HH_OK) return rc;
     if (e != cudaSuccess) return cuda_fail(e, "factorisation", __FILE__, __LINE__);
     return HH_OK;
@@ -489,7 +506,7 @@ extern "C" int hh_plan3d_create_helmholtz(hh_ctx *x, int n, int order, double kr
 extern "C" int hh_plan_destroy(hh_plan *pl) {
     if (!pl) return HH_OK;
     cudaSetDevice(pl->p.ctx->device);
-    cudaStreamSynchronize(pl->p.ctx->stream);
+    if (!pl->p.ctx->pool) cudaStreamSynchronize(pl->p.ctx->stream); // pool frees are stream-ordered
     plan_free(pl);
     delete pl;
     return HH_OK;

@@ -80,6 +80,8 @@ struct Ctx {
     long long                timed_solves = 0;
     // host-buffer solves: copy streams and per-chunk events (created on first use)
     cudaStream_t             copy_in = nullptr, copy_out = nullptr;
+    // plan memory pool (set by the request loop; null = cudaMalloc/cudaFree, synchronous set-up)
+    cudaMemPool_t            pool = nullptr;
     std::vector<cudaEvent_t> chunk_ev;
 };
 

@@ -61,6 +61,8 @@ struct hh_server {
     int                                 device = 0;
     hh_ctx                             *ctx = nullptr;
     std::vector<cudaStream_t>           streams;
+    cudaStream_t                        setup = nullptr;   // plan set-up (asynchronous)
+    cudaEvent_t                         ready = nullptr;   // set-up done, per plan creation
     cudaMemPool_t                       pool = nullptr;
     int                                *flags = nullptr; // pinned, one slot per stream
     size_t                              budget = 0, used = 0;
@@ -168,7 +170,7 @@ std::vector<hh_plan *> pick_victims(hh_server *s, size_t need) {
 }
 
 // Enqueue the batch on the next stream.  On failure nothing of it is left in flight.
-int run_batch(hh_server *s, Batch *b, hh_plan *plan) {
+int run_batch(hh_server *s, Batch *b, hh_plan *plan, cudaEvent_t after) {
     const hh_request &r0 = b->reqs[0]->r;
     const long        field = points_of(r0);
     const int         si = s->rr++ % (int)s->streams.size();
@@ -176,6 +178,7 @@ int run_batch(hh_server *s, Batch *b, hh_plan *plan) {
     double2          *buf = nullptr;
     auto enqueue = [&]() -> int {
         HH_TRY(hh_ctx_set_stream(s->ctx, st));
+        if (after) HH_CUDA(cudaStreamWaitEvent(st, after, 0)); // the plan's set-up
         int total = 0;
         for (Req *q : b->reqs) total += q->r.nrhs;
         if (b->staging == 0) {
@@ -250,6 +253,7 @@ void dispatcher(hh_server *s) {
         std::vector<hh_plan *> victims = pick_victims(s, need());
         if (!victims.empty()) {
             lk.unlock();
+            hh_ctx_set_stream(s->ctx, s->setup); // idle plans: their memory returns to the pool in order
             for (hh_plan *v : victims) hh_plan_destroy(v);
             lk.lock();
         }
@@ -271,12 +275,18 @@ void dispatcher(hh_server *s) {
         s->used += b->staging + pbytes; // staging and (reserved) plan memory
         b->reserved = true;
         hh_plan *plan = nullptr;
+        bool fresh = false;
         if (create) {
-            lk.unlock(); // plan set-up synchronizes its stream
+            lk.unlock();
+            // asynchronous set-up on its own stream; the batch waits for it with an event
             const hh_request &r = head->r;
-            const int rc = r.dim == 2 ? hh_plan2d_create_helmholtz(s->ctx, r.n, r.order, r.k_re, r.k_im, &plan)
-                                      : hh_plan3d_create_helmholtz(s->ctx, r.n, r.order, r.k_re, r.k_im, &plan);
+            int rc = hh_ctx_set_stream(s->ctx, s->setup);
+            if (rc == HH_OK)
+                rc = r.dim == 2 ? hh_plan2d_create_helmholtz(s->ctx, r.n, r.order, r.k_re, r.k_im, &plan)
+                                : hh_plan3d_create_helmholtz(s->ctx, r.n, r.order, r.k_re, r.k_im, &plan);
+            if (rc == HH_OK && cudaEventRecord(s->ready, s->setup) != cudaSuccess) rc = HH_ERR_CUDA;
             const std::string msg = rc == HH_OK ? std::string() : std::string(hh_last_error());
+            fresh = rc == HH_OK;
             lk.lock();
             if (rc != HH_OK) {
                 s->used -= pbytes;
@@ -296,7 +306,7 @@ void dispatcher(hh_server *s) {
         plan = pe.plan;
         b->plan_ref = true;
         lk.unlock();
-        const int rc = run_batch(s, b, plan);
+        const int rc = run_batch(s, b, plan, fresh ? s->ready : nullptr);
         if (rc != HH_OK) fail_batch(s, b, rc, hh_last_error());
         lk.lock();
     }
@@ -333,6 +343,9 @@ extern "C" int hh_server_create(int device, size_t budget, int streams, hh_serve
     }
     if (e == cudaSuccess) e = cudaHostAlloc((void **)&s->flags, sizeof(int) * 64, cudaHostAllocDefault);
     if (e == cudaSuccess) memset(s->flags, 0, sizeof(int) * 64);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->setup, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) reinterpret_cast<hh::Ctx *>(s->ctx)->pool = s->pool;
     for (int i = 0; i < streams && e == cudaSuccess; i++) {
         cudaStream_t st;
         e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
@@ -421,8 +434,11 @@ extern "C" int hh_server_destroy(hh_server *s) {
     }
     for (auto &kv : s->plans) hh_plan_destroy(kv.second.plan);
     for (auto &kv : s->reqs) delete kv.second;
+    cudaStreamSynchronize(s->setup);
     hh_ctx_destroy(s->ctx); // while its current stream (one of the server's) still exists
     for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
+    cudaStreamDestroy(s->setup);
+    cudaEventDestroy(s->ready);
     cudaMemPoolDestroy(s->pool);
     cudaFreeHost(s->flags);
     delete s;
