@@ -67,6 +67,7 @@ SIGNATURES = {
     "hh_solve_host": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source_host": (_i, [_vp, _vp, _vp, _i]),
+    "hh_solve_source_host_noalloc": (_i, [_vp, _vp, _vp, _i]),
     "hh_coefficients2d": (_i, [_i, _i, _d, _d, C.POINTER(_vp)]),
     "hh_coefficients3d": (_i, [_i, _i, _d, _d, C.POINTER(_vp)]),
     "hh_ctx_set_stage_timing": (_i, [_vp, _i]),
@@ -249,6 +250,15 @@ class Plan:
         batch = rhs.size // self.field
         out = np.empty_like(rhs)
         check(lib().hh_solve_host(self.h, rhs.ctypes.data, out.ctypes.data, batch), "hh_solve_host")
+        return out
+
+    def solve_source_host_noalloc(self, f: np.ndarray) -> np.ndarray:
+        """hh_solve_source_host_noalloc: staging in the library's fixed 32 MiB device array."""
+        f = np.ascontiguousarray(f, dtype=np.complex128)
+        batch = f.size // self.field
+        out = np.empty_like(f)
+        check(lib().hh_solve_source_host_noalloc(self.h, f.ctypes.data, out.ctypes.data, batch),
+              "hh_solve_source_host_noalloc")
         return out
 
     def solve_source_host(self, f: np.ndarray) -> np.ndarray:

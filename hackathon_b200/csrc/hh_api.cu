@@ -17,6 +17,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
 #include <string>
 
 struct hh_ctx {
@@ -703,4 +704,45 @@ extern "C" int hh_solve_host(hh_plan *pl, const double *rhs, double *sol, int ba
 }
 extern "C" int hh_solve_source_host(hh_plan *pl, const double *f, double *u, int batch) {
     return solve_host_common(pl, f, u, batch, true);
+}
+
+// ------------------------------------------------------ allocation-free host solve ------
+// Device staging for hh_solve_source_host_noalloc: one file-scope array per device, 32 MiB
+// (2^21 complex values: e.g. two 1023^2 right-hand sides or one 127^3).  Nothing in it has to
+// start at zero: every call writes each element it reads.  Calls that overlap in time on one
+// device share it and race; they must be serialized.
+constexpr long kNoAllocElems = 1L << 21;
+static __device__ __align__(256) double2 g_noalloc_stage[kNoAllocElems];
+
+extern "C" int hh_solve_source_host_noalloc(hh_plan *pl, const double *f_host, double *u_host, int batch) {
+    HH_TRY(check_batch(pl, batch));
+    if (batch == 0) return HH_OK;
+    if (!f_host || !u_host) { set_error("hh_solve_source_host_noalloc: null buffer"); return HH_ERR_INVALID; }
+    Plan &p = pl->p;
+    if (p.src_order == 0) {
+        set_error("hh_solve_source_host_noalloc needs a plan from hh_plan{2,3}d_create_helmholtz");
+        return HH_ERR_INVALID;
+    }
+    if (p.field * (long)batch > kNoAllocElems) {
+        set_error("hh_solve_source_host_noalloc: %ld complex values exceed the %ld-value staging area",
+                  p.field * (long)batch, kNoAllocElems);
+        return HH_ERR_UNSUPPORTED;
+    }
+    Ctx *c = p.ctx;
+    HH_CUDA(cudaSetDevice(c->device));
+    // the staging address, looked up once per device
+    static std::mutex mu;
+    static double2   *addr[64] = {};
+    double2          *d = nullptr;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        if (c->device < 0 || c->device >= 64) { set_error("device %d", c->device); return HH_ERR_INVALID; }
+        if (!addr[c->device]) HH_CUDA(cudaGetSymbolAddress((void **)&addr[c->device], g_noalloc_stage));
+        d = addr[c->device];
+    }
+    const size_t bytes = sizeof(double2) * (size_t)p.field * batch;
+    HH_CUDA(cudaMemcpyAsync(d, f_host, bytes, cudaMemcpyHostToDevice, c->stream));
+    HH_TRY(hh_solve_source(pl, (const double *)d, (double *)d, batch));
+    HH_CUDA(cudaMemcpyAsync(u_host, d, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return hh_ctx_synchronize(reinterpret_cast<hh_ctx *>(c)); // Ctx is the first member of hh_ctx
 }

@@ -124,6 +124,14 @@ int hh_solve_host(hh_plan *plan, const double *rhs_host, double *sol_host, int b
  * 2D_Program/main_functions/rhs.c:100, 3D_Program/main_functions/rhs.c:198, for this class). */
 int hh_solve_source(hh_plan *plan, const double *f_dev, double *u_dev, int batch);
 int hh_solve_source_host(hh_plan *plan, const double *f_host, double *u_host, int batch);
+/* The same host-buffer solve without any allocation (no counterpart in the reference).  For
+ * callers that must not allocate device memory while they run, e.g. with a fixed memory budget
+ * or where allocator latency is unwelcome: the device staging is a 32 MiB array of the library
+ * (2^21 complex values, so field size * batch <= 2097152, e.g. two 1023^2 or one 127^3
+ * right-hand sides; larger requests fail with HH_ERR_UNSUPPORTED).  The first call on a device
+ * looks up the array's address; make it before any stream capture.  The array is shared by all
+ * contexts on a device: calls that overlap in time race and must be serialized by the caller. */
+int hh_solve_source_host_noalloc(hh_plan *plan, const double *f_host, double *u_host, int batch);
 
 /* Stencil coefficients the Helmholtz plans use (host arrays of n complex values each):
  * 2D order in bp,ap,b,a,bm,am order; 3D in a..dm order (12 arrays). */

@@ -1,0 +1,36 @@
+"""hh_solve_source_host_noalloc: the host-buffer solve with its staging in the library's fixed
+device array.  Collected last (file name), so it also runs after every other GPU test."""
+import numpy as np
+import pytest
+
+import hackathon_b200 as hh
+from hackathon_b200 import workload as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _f(n, seed):
+    return W.source_2d(n, W.sine_modes(seed, 8, 20), noise_seed=seed + 1, noise_var=1e-3)[1:-1, 1:-1]
+
+
+@pytest.mark.parametrize("n,order,k,batch", [(1023, 6, 50.0, 2), (511, 4, 100.0, 8), (255, 6, 10.0, 5)])
+def test_noalloc_equals_allocating_solve_twice(ctx, n, order, k, batch):
+    plan = hh.Plan.helmholtz(ctx, 2, n, order, k)
+    for call in range(2):  # two calls in a row: nothing carries over between them
+        f = np.stack([_f(n, 100 * call + b) for b in range(batch)])
+        want = plan.solve_source_host(f)
+        got = plan.solve_source_host_noalloc(f)
+        assert np.array_equal(got, want)
+    plan.close()
+
+
+def test_noalloc_3d_and_rejection(ctx):
+    n = 63
+    plan = hh.Plan.helmholtz(ctx, 3, n, 6, 30.0)
+    f = W.source_3d(n, W.sine_modes(9, 8, 16, dim=3))[1:-1, 1:-1, 1:-1]
+    assert np.array_equal(plan.solve_source_host_noalloc(f), plan.solve_source_host(f))
+    plan.close()
+    big = hh.Plan.helmholtz(ctx, 2, 1023, 6, 50.0)
+    with pytest.raises(hh.HHError, match="HH_ERR_UNSUPPORTED"):
+        big.solve_source_host_noalloc(np.zeros((3, 1023, 1023), dtype=np.complex128))  # over 2^21 values
+    big.close()
