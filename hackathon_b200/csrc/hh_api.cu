@@ -268,6 +268,10 @@ static int plan_alloc(hh_plan *pl) {
     HH_TRY(dalloc(c, (void **)&p.subt, sizeof(double2) * 4 * (size_t)p.prow));
     HH_TRY(dalloc(c, (void **)&p.diagt, sizeof(double2) * 4 * (size_t)p.prow));
     HH_TRY(dalloc(c, (void **)&p.mu, sizeof(double) * 3 * (size_t)p.lines));
+    // the context's transform tables for this plan's lengths are made here, at set-up, so that
+    // solving never allocates
+    HH_TRY(prepare_dst(c, p.nx));
+    if (p.dim == 3) HH_TRY(prepare_dst(c, p.ny));
     return HH_OK;
 }
 

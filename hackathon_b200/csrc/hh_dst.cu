@@ -880,6 +880,20 @@ int tables_for(Ctx *c, int m, const double2 **tw, const double **sn) {
     return HH_OK;
 }
 
+int prepare_dst(Ctx *c, int n) {
+    const int m = n + 1;
+    if (m >= 64 && m <= 8192 && (m & (m - 1)) == 0) {
+        const double2 *tw;
+        const double  *sn;
+        return tables_for(c, m, &tw, &sn);
+    }
+    if (n >= 1 && n <= 4096) {
+        const double *mat;
+        return dense_for(c, n, &mat);
+    }
+    return HH_OK; // lengths the transforms refuse fail at solve time
+}
+
 int dense_for(Ctx *c, int n, const double **mat) {
     std::lock_guard<std::mutex> g(c->mu);
     auto it = c->dense.find(n);

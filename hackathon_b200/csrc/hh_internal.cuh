@@ -87,6 +87,8 @@ struct Ctx {
 
 int tables_for(Ctx *c, int m, const double2 **tw, const double **sn);
 int dense_for(Ctx *c, int n, const double **mat);
+// builds (once per context) the tables that DSTs of length n use
+int prepare_dst(Ctx *c, int n);
 
 // Plan: one (dim, sizes, stencil coefficients) problem with its device-resident setup.
 struct Plan {

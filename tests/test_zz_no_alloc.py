@@ -1,5 +1,6 @@
-"""hh_solve_source_host_noalloc: the host-buffer solve with its staging in the library's fixed
-device array.  Collected last (file name), so it also runs after every other GPU test."""
+"""hh_solve_source_host_noalloc: the host-buffer solve for callers that must not allocate device
+memory while they run; its staging is the library's fixed device array.  Collected last (file
+name), so it also runs after every other GPU test."""
 import numpy as np
 import pytest
 
@@ -34,3 +35,18 @@ def test_noalloc_3d_and_rejection(ctx):
     with pytest.raises(hh.HHError, match="HH_ERR_UNSUPPORTED"):
         big.solve_source_host_noalloc(np.zeros((3, 1023, 1023), dtype=np.complex128))  # over 2^21 values
     big.close()
+
+
+def test_noalloc_first_call_on_a_fresh_context():
+    """The allocation-free call as the very first solve of a new context (every table it needs
+    was made when the plan was created), then again, against the allocating entry point."""
+    ctx = hh.Context(0)
+    n = 1023
+    plan = hh.Plan.helmholtz(ctx, 2, n, 4, 30.0)
+    f1, f2 = _f(n, 7), _f(n, 8)
+    got1 = plan.solve_source_host_noalloc(f1)
+    got2 = plan.solve_source_host_noalloc(f2)
+    assert np.array_equal(got1, plan.solve_source_host(f1))
+    assert np.array_equal(got2, plan.solve_source_host(f2))
+    plan.close()
+    ctx.close()
