@@ -28,7 +28,7 @@ CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall"]
 
 CU_SOURCES = ["hh_api.cu", "hh_dst.cu", "hh_tridiag.cu", "hh_server.cu"]
 C_SOURCES = ["hh_coef.c"]
-HEADERS = ["hh_internal.cuh"]
+HEADERS = ["hh_internal.cuh", "hh_tma.cuh"]
 
 
 def _nvcc() -> str:

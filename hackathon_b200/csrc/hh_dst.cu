@@ -26,6 +26,7 @@
 // through shared memory rather than warp shuffles: a shuffle moves 32 bits, so a complex
 // double costs four shuffles per hop.
 #include "hh_internal.cuh"
+#include "hh_tma.cuh"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -139,55 +140,6 @@ template <int T> __device__ __forceinline__ void slot_sync(int slot) {
     } else {
         asm volatile("bar.sync %0, %1;" ::"r"(slot + 1), "r"(T) : "memory");
     }
-}
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-// 1D bulk copy global -> shared completing on `bar` (addresses 16-byte aligned, size % 16 == 0)
-__device__ __forceinline__ void tma_bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-// bounded wait on phase 0; returns false if the copy did not land within the budget
-__device__ __forceinline__ bool mbar_wait0(uint64_t *bar) {
-    const uint32_t a = smem_u32(bar);
-    for (long it = 0; it < (1L << 26); it++) {
-        uint32_t done;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(done)
-            : "r"(a)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-// bounded wait on an mbarrier phase; false if it did not complete within the budget
-__device__ __forceinline__ bool mbar_wait_parity(uint64_t *bar, uint32_t parity) {
-    const uint32_t a = smem_u32(bar);
-    for (long it = 0; it < (1L << 26); it++) {
-        uint32_t done;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(done)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
 }
 
 // one Stockham pass of radix RAD at stride NS over the padded slot buffer
@@ -1009,6 +961,15 @@ int launch_dst_rows(Ctx *c, int n, long rows, const double2 *in, long in_ld, dou
 // columns by `box_rows` rows.
 static int encode_col_map(CUtensorMap *map, const double2 *base, long ncols, long rows, long planes, long ld,
                           long plane_stride, int box_cols, int box_rows) {
+    const unsigned long long dims[4] = {2, (unsigned long long)ncols, (unsigned long long)rows,
+                                        (unsigned long long)planes};
+    const unsigned long long strides[3] = {16, (unsigned long long)ld * 16, (unsigned long long)plane_stride * 16};
+    const unsigned           box[4] = {2, (unsigned)box_cols, (unsigned)box_rows, 1};
+    return encode_tensor_map(map, base, 4, dims, strides, box);
+}
+
+int encode_tensor_map(CUtensorMap *map, const void *base, int rank, const unsigned long long *dims,
+                      const unsigned long long *strides, const unsigned *box) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
         cudaDriverEntryPointQueryResult q;
@@ -1020,13 +981,16 @@ static int encode_col_map(CUtensorMap *map, const double2 *base, long ncols, lon
         }
         encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
     }
-    const cuuint64_t dims[4] = {2, (cuuint64_t)ncols, (cuuint64_t)rows, (cuuint64_t)planes};
-    const cuuint64_t strides[3] = {16, (cuuint64_t)ld * 16, (cuuint64_t)plane_stride * 16};
-    const cuuint32_t box[4] = {2, (cuuint32_t)box_cols, (cuuint32_t)box_rows, 1};
-    const cuuint32_t estr[4] = {1, 1, 1, 1};
-    const CUresult   r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double2 *>(base), dims, strides, box,
-                                estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    cuuint64_t d[5], s[4];
+    cuuint32_t b[5], e[5] = {1, 1, 1, 1, 1};
+    for (int i = 0; i < rank; i++) {
+        d[i] = dims[i];
+        b[i] = box[i];
+        if (i + 1 < rank) s[i] = strides[i];
+    }
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (cuuint32_t)rank, const_cast<void *>(base), d, s, b, e,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
         return HH_ERR_CUDA;

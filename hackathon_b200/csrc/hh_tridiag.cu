@@ -485,7 +485,7 @@ struct SolveVariant {
     int nt, minb;
 };
 static const SolveVariant kVariants[] = {{512, 1}, {256, 2}};
-constexpr int kNumVariants = 2; // plus variants 2..4: k_line_solve_sym where the plan allows it
+constexpr int kNumVariants = 2; // plus variants 2..5: k_line_solve_sym where the plan allows it
 
 // segments per line: a power of two >= NT/32 (so at most 32 lines share a warp)
 static int solve_geometry(int rows, int nt, int *CW, int *P) {
@@ -509,7 +509,7 @@ int padded_rows(int rows) {
     return best;
 }
 
-int solve_variant_count() { return kNumVariants + 3; }
+int solve_variant_count() { return kNumVariants + 4; }
 
 template <int SRC, bool CR, int NT, int MINB>
 static int launch_solve_t(Plan *p, const double2 *in, double2 *out, int batch) {
@@ -666,17 +666,17 @@ struct SymParams {
 // One chunk of right-hand sides for the thread's segment, NR of them side by side (independent
 // dependency chains, shared barriers).  TINT = the warp's rows all lie in [9, rows) (constant
 // Pade factors).
-template <int SRC, int NT, int CW, bool TINT, int NR>
+template <int SRC, int NT, int CW, bool TINT, int NR, int KS>
 __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double2 *__restrict__ out, int rows,
                                           long row_stride, long field, int b_begin, int b_end, long off0,
-                                          bool live, int r0, int sl, int w, int c, const double2 (&Lr)[kSeg],
-                                          const double2 (&ui)[kSeg], double2 ui_in, double2 s, double2 c1, double c2,
+                                          bool live, int r0, int sl, int w, int c, const double2 (&Lr)[KS],
+                                          const double2 (&ui)[KS], double2 ui_in, double2 s, double2 c1, double c2,
                                           double2 cT, SymSmem<NT / 32, CW, NR> &sm, double2 *pre,
                                           const double2 *tabF, const double2 *tabB, const double *ttF,
                                           const double *ttB, const SymParams &sp) {
     constexpr int NW = NT / 32, SPW = 32 / CW, LOG = ilog2_t<SPW>();
     constexpr int HALO = (SRC == 4 || SRC == 6) ? 1 : 0;
-    constexpr int SLOTS = kSeg + 2;
+    constexpr int SLOTS = KS + 2;
     // cross-warp sequential passes: main solve on threads [0, CW NR), Pade solve on [128, 128 + CW NR)
     static_assert(CW * NR <= 128 && NT >= 256, "cross-warp thread ranges");
     const int     t = threadIdx.x;
@@ -706,7 +706,7 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
             const bool     okb = live && b + r < b_end;
             const double2 *src = in + (long)(okb ? b + r : 0) * field + off0;
 #pragma unroll
-            for (int k = -HALO; k < kSeg + HALO; k++) {
+            for (int k = -HALO; k < KS + HALO; k++) {
                 const bool ok = okb && r0 + k >= 0 && r0 + k < rows;
                 cp_async16(&pre[(r * SLOTS + k + 1) * NT + t], ok ? src + (long)k * row_stride : in, ok ? 16 : 0);
             }
@@ -715,17 +715,17 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
     };
     prefetch(b_begin);
     for (int b = b_begin; b < b_end; b += NR) {
-        double2 v[NR][kSeg], g[NR][kSeg], gm[NR], gp[NR];
+        double2 v[NR][KS], g[NR][KS], gm[NR], gp[NR];
         cp_async_wait_all();
 #pragma unroll
         for (int r = 0; r < NR; r++) {
 #pragma unroll
-            for (int k = 0; k < kSeg; k++) v[r][k] = pre[(r * SLOTS + k + 1) * NT + t];
+            for (int k = 0; k < KS; k++) v[r][k] = pre[(r * SLOTS + k + 1) * NT + t];
             gm[r] = zero;
             gp[r] = zero;
             if constexpr (HALO) {
                 gm[r] = pre[(r * SLOTS) * NT + t];
-                gp[r] = pre[(r * SLOTS + kSeg + 1) * NT + t];
+                gp[r] = pre[(r * SLOTS + KS + 1) * NT + t];
             }
         }
         if (b + NR < b_end) prefetch(b + NR);
@@ -735,12 +735,12 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
         for (int r = 0; r < NR; r++) {
             if constexpr (SRC == 2) {
 #pragma unroll
-                for (int k = 0; k < kSeg; k++) v[r][k] = cscale(v[r][k], sp.h2);
+                for (int k = 0; k < KS; k++) v[r][k] = cscale(v[r][k], sp.h2);
             } else if constexpr (SRC == 4 || SRC == 6) {
                 double2 prev = gm[r];
 #pragma unroll
-                for (int k = 0; k < kSeg; k++) {
-                    const double2 gk = v[r][k], nx = (k == kSeg - 1) ? gp[r] : v[r][k + 1];
+                for (int k = 0; k < KS; k++) {
+                    const double2 gk = v[r][k], nx = (k == KS - 1) ? gp[r] : v[r][k + 1];
                     const double2 d2 = make_double2(fma(-2.0, gk.x, prev.x + nx.x), fma(-2.0, gk.y, prev.y + nx.y));
                     prev = gk;
                     if constexpr (SRC == 6) g[r][k] = gk;
@@ -754,7 +754,7 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
 #pragma unroll
         for (int r = 0; r < NR; r++) { yh[r] = zero; zh[r] = zero; }
 #pragma unroll
-        for (int k = 0; k < kSeg; k++) {
+        for (int k = 0; k < KS; k++) {
             const double2 l = LF(k);
 #pragma unroll
             for (int r = 0; r < NR; r++) {
@@ -808,7 +808,7 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
                 if constexpr (SRC == 6) z[r] = zaxpy(bfe[r], aeF, sm.eF[r][w][c]);
             }
 #pragma unroll
-            for (int k = 0; k < kSeg; k++) {
+            for (int k = 0; k < KS; k++) {
                 const double2 l = LF(k);
 #pragma unroll
                 for (int r = 0; r < NR; r++) {
@@ -827,7 +827,7 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
 #pragma unroll
         for (int r = 0; r < NR; r++) { xh[r] = zero; wh[r] = zero; }
 #pragma unroll
-        for (int k = kSeg - 1; k >= 0; k--) {
+        for (int k = KS - 1; k >= 0; k--) {
 #pragma unroll
             for (int r = 0; r < NR; r++) {
                 xh[r] = cmul(ui[k], zfms(v[r][k], s, xh[r]));
@@ -880,7 +880,7 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
                 if constexpr (SRC == 6) ww[r] = zaxpy(bbe[r], aeB, sm.eB[r][w][c]);
             }
 #pragma unroll
-            for (int k = kSeg - 1; k >= 0; k--) {
+            for (int k = KS - 1; k >= 0; k--) {
 #pragma unroll
                 for (int r = 0; r < NR; r++) {
                     x[r] = cmul(ui[k], zfms(v[r][k], s, x[r]));
@@ -898,7 +898,7 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
             if (b + r >= b_end) break;
             double2 *dst = out + (long)(b + r) * field + off0;
 #pragma unroll
-            for (int k = 0; k < kSeg; k++)
+            for (int k = 0; k < KS; k++)
                 if (live && r0 + k < rows) dst[(long)k * row_stride] = v[r][k];
         }
     }
@@ -931,7 +931,7 @@ __device__ __forceinline__ M sym_scan_table(M a, M *tab, int NT_, int sl, M one)
     return a;
 }
 
-template <int SRC, int NT, int CW, int MINB, int NR>
+template <int SRC, int NT, int CW, int MINB, int NR, int KS>
 __global__ void __launch_bounds__(NT, MINB)
     k_line_solve_sym(const double2 *__restrict__ in, double2 *__restrict__ out, int lines, int rows, long row_stride,
                      long field, int batch, int rb, const double2 *__restrict__ Pv, const double2 *__restrict__ subt,
@@ -940,8 +940,8 @@ __global__ void __launch_bounds__(NT, MINB)
     constexpr int HALO = (SRC == 4 || SRC == 6) ? 1 : 0;
     __shared__ SymSmem<NW, CW, NR> sm;
     extern __shared__ double2 dyn[];
-    double2 *pre = dyn;                                 // [NR][kSeg + 2][NT]
-    double2 *tabF = pre + NR * (kSeg + 2) * NT;         // [LOG + 1][NT]
+    double2 *pre = dyn;                                 // [NR][KS + 2][NT]
+    double2 *tabF = pre + NR * (KS + 2) * NT;         // [LOG + 1][NT]
     double2 *tabB = tabF + (LOG + 1) * NT;              // [LOG + 1][NT]
     double  *ttF = reinterpret_cast<double *>(tabB + (LOG + 1) * NT); // [LOG + 1][NT] (order 6)
     double  *ttB = ttF + (LOG + 1) * NT;
@@ -952,19 +952,19 @@ __global__ void __launch_bounds__(NT, MINB)
     const int q = blockIdx.x * CW + c;
     const bool live = q < lines;
     const int  qq = live ? q : 0;
-    const int  r0 = seg * kSeg;
+    const int  r0 = seg * KS;
     const double m0 = mu[qq], m1 = mu[lines + qq], m2 = mu[2 * lines + qq];
     const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
 
     // ---- factors of the thread's rows (the set-up's recurrence, same arithmetic)
     const double2 s = shifted(subt, prow, 0, m0, m1, m2), d = shifted(diagt, prow, 0, m0, m1, m2);
-    double2 Lr[kSeg], ui[kSeg];
+    double2 Lr[KS], ui[KS];
     double2 Af = one, Ab = one;
-    const double2 ui_in = (live && r0 > 0 && r0 < rows) ? Pv[(long)seg * lines + q] : zero; // 1/P of row r0-1
+    const double2 ui_in = (live && r0 > 0 && r0 < rows) ? Pv[(long)(r0 / 8) * lines + q] : zero; // 1/P of row r0-1
     {
         double2 uprev = ui_in;
 #pragma unroll
-        for (int k = 0; k < kSeg; k++) {
+        for (int k = 0; k < KS; k++) {
             const int r = r0 + k;
             Lr[k] = zero;
             ui[k] = zero;
@@ -1021,7 +1021,7 @@ __global__ void __launch_bounds__(NT, MINB)
         __syncthreads();
         double af = 1.0, ab = 1.0;
 #pragma unroll
-        for (int k = 0; k < kSeg; k++) {
+        for (int k = 0; k < KS; k++) {
             const int r = r0 + k;
             af *= -(r < 9 ? sm.pl[r] : (r < rows ? sp.linf : 0.0));
             ab *= -(r < 9 ? sm.pu[r] : (r < rows ? sp.uinf : 0.0));
@@ -1037,12 +1037,12 @@ __global__ void __launch_bounds__(NT, MINB)
     const int  b_end = min(batch, b_begin + rb);
     const long off0 = (long)r0 * row_stride + qq;
     // warps whose rows all lie in [9, rows) use the constant Pade factors
-    const bool tint = (w * SPW * kSeg >= 9) && ((w + 1) * SPW * kSeg <= rows);
+    const bool tint = (w * SPW * KS >= 9) && ((w + 1) * SPW * KS <= rows);
     if (SRC == 6 && tint)
-        sym_chunk<SRC, NT, CW, true, NR>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0, sl, w, c, Lr,
+        sym_chunk<SRC, NT, CW, true, NR, KS>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0, sl, w, c, Lr,
                                      ui, ui_in, s, c1, c2, cT, sm, pre, tabF, tabB, ttF, ttB, sp);
     else
-        sym_chunk<SRC, NT, CW, false, NR>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0, sl, w, c, Lr,
+        sym_chunk<SRC, NT, CW, false, NR, KS>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0, sl, w, c, Lr,
                                       ui, ui_in, s, c1, c2, cT, sm, pre, tabF, tabB, ttF, ttB, sp);
 }
 
@@ -1062,7 +1062,7 @@ static int pick_rb(long groups, int batch, int resident, int nr) {
     return best;
 }
 
-template <int SRC, int CW, int MINB, int NR>
+template <int SRC, int CW, int MINB, int NR, int KS>
 static int launch_sym_t(Plan *p, const double2 *in, double2 *out, int batch) {
     constexpr int NT = 256, SPW = 32 / CW, LOG = ilog2_t<SPW>();
     SymParams sp;
@@ -1073,52 +1073,55 @@ static int launch_sym_t(Plan *p, const double2 *in, double2 *out, int batch) {
     sp.uinf = p->pade_uinf;
     sp.pl = p->pade_l;
     sp.pu = p->pade_u;
-    const int shm = (int)(sizeof(double2) * (NR * (kSeg + 2) * NT + 2 * (LOG + 1) * NT) +
+    const int shm = (int)(sizeof(double2) * (NR * (KS + 2) * NT + 2 * (LOG + 1) * NT) +
                           (SRC == 6 ? sizeof(double) * 2 * (LOG + 1) * NT : 0));
-    HH_CUDA(cudaFuncSetAttribute(k_line_solve_sym<SRC, NT, CW, MINB, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    HH_CUDA(cudaFuncSetAttribute(k_line_solve_sym<SRC, NT, CW, MINB, NR, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  shm));
     const long groups = (p->lines + CW - 1) / CW;
     int blocks_per_sm = 0, dev = 0, sms = 148;
-    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_line_solve_sym<SRC, NT, CW, MINB, NR>, NT,
+    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_line_solve_sym<SRC, NT, CW, MINB, NR, KS>, NT,
                                                           shm));
     HH_CUDA(cudaGetDevice(&dev));
     HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int rb = pick_rb(groups, batch, std::max(1, blocks_per_sm) * sms, NR);
     const int chunks = (batch + rb - 1) / rb;
     dim3 grid((unsigned)groups, (unsigned)chunks);
-    k_line_solve_sym<SRC, NT, CW, MINB, NR><<<grid, NT, shm, p->ctx->stream>>>(
+    k_line_solve_sym<SRC, NT, CW, MINB, NR, KS><<<grid, NT, shm, p->ctx->stream>>>(
         in, out, p->lines, p->rows, p->row_stride, p->field, batch, rb, p->Pv, p->subt, p->diagt, p->prow, p->mu, sp);
     HH_CUDA(cudaGetLastError());
     p->ctx->launches++;
     return HH_OK;
 }
 
-template <int SRC, int MINB, int NR> static int launch_sym_src(Plan *p, const double2 *in, double2 *out, int batch) {
-    // segments per line: a power of two P >= rows / kSeg with 8 <= P <= 256 (CW = 256 / P lines per CTA)
+template <int SRC, int MINB, int NR, int KS> static int launch_sym_src(Plan *p, const double2 *in, double2 *out, int batch) {
+    // segments per line: a power of two P >= rows / KS with 8 <= P <= 256 (CW = 256 / P lines per CTA)
     int P = 8;
-    while (P * kSeg < p->rows) P <<= 1;
+    while (P * KS < p->rows) P <<= 1;
     switch (P) {
-    case 8: return launch_sym_t<SRC, 32, MINB, 1>(p, in, out, batch); // per-RHS scan arrays would not fit
-    case 16: return launch_sym_t<SRC, 16, MINB, NR>(p, in, out, batch);
-    case 32: return launch_sym_t<SRC, 8, MINB, NR>(p, in, out, batch);
-    case 64: return launch_sym_t<SRC, 4, MINB, NR>(p, in, out, batch);
-    case 128: return launch_sym_t<SRC, 2, MINB, NR>(p, in, out, batch);
-    case 256: return launch_sym_t<SRC, 1, MINB, NR>(p, in, out, batch);
+    case 8: return launch_sym_t<SRC, 32, MINB, 1, KS>(p, in, out, batch); // per-RHS scan arrays would not fit
+    case 16: return launch_sym_t<SRC, 16, MINB, NR, KS>(p, in, out, batch);
+    case 32: return launch_sym_t<SRC, 8, MINB, NR, KS>(p, in, out, batch);
+    case 64: return launch_sym_t<SRC, 4, MINB, NR, KS>(p, in, out, batch);
+    case 128: return launch_sym_t<SRC, 2, MINB, NR, KS>(p, in, out, batch);
+    case 256: return launch_sym_t<SRC, 1, MINB, NR, KS>(p, in, out, batch);
     default: set_error("symmetric line solve: %d rows", p->rows); return HH_ERR_UNSUPPORTED;
     }
 }
 
 bool sym_solve_supported(const Plan *p, int src_order) {
-    return p->sym && p->rows <= 256 * kSeg && (src_order != 6 || (p->pf_ok && p->pade_l));
+    const int max_rows = 256 * (p->variant == 5 ? 16 : kSeg);
+    return p->sym && p->rows <= max_rows && (src_order != 6 || (p->pf_ok && p->pade_l));
 }
 
 // Variants of the symmetric kernel: 2 = two CTAs per SM, 3 = one CTA per SM (no register cap),
-// 4 = one CTA per SM with two right-hand sides per pass.
+// 4 = one CTA per SM with two right-hand sides per pass, 5 = one CTA per SM with 16-row segments
+// (twice the lines per CTA: wider contiguous row pieces in global memory, half the scans).
 template <int SRC> static int launch_sym_variant(Plan *p, const double2 *in, double2 *out, int batch) {
     switch (p->variant) {
-    case 3: return launch_sym_src<SRC, 1, 1>(p, in, out, batch);
-    case 4: return launch_sym_src<SRC, 1, 2>(p, in, out, batch);
-    default: return launch_sym_src<SRC, 2, 1>(p, in, out, batch);
+    case 3: return launch_sym_src<SRC, 1, 1, kSeg>(p, in, out, batch);
+    case 4: return launch_sym_src<SRC, 1, 2, kSeg>(p, in, out, batch);
+    case 5: return launch_sym_src<SRC, 1, 1, 16>(p, in, out, batch);
+    default: return launch_sym_src<SRC, 2, 1, kSeg>(p, in, out, batch);
     }
 }
 

@@ -69,26 +69,26 @@ def test_batch_equals_single(ctx, oracle):
 @pytest.mark.parametrize("n,order,k", [(15, 6, 10.0), (31, 6, 10.0), (63, 2, 30.0), (255, 4, 50.0), (511, 6, 20.0),
                                        (1023, 6, 50.0), (1023, 4, 10.0), (2047, 6, 100.0)])
 def test_every_line_solve_variant_matches_oracle(ctx, oracle, n, order, k):
-    """Each line-solve kernel on its own (0/1: general rows, 512 or 256 threads; 2/3/4: symmetric
-    constant rows with the order-6 partial fractions, 2 or 1 blocks per SM, one or two right-hand
-    sides per pass), then hh_plan_tune's choice."""
+    """Each line-solve kernel on its own (0/1: general rows, 512 or 256 threads; 2..5: symmetric
+    constant rows with the order-6 partial fractions -- 2 or 1 blocks per SM, one or two
+    right-hand sides per pass, 8- or 16-row segments), then hh_plan_tune's choice."""
     f = _source(n, 7 * n + order)
     ref = oracle.pipeline_2d(n, order, k, f)
     plan = hh.Plan.helmholtz(ctx, 2, n, order, k)
     assert plan.variant == 2  # constant k: the symmetric kernel by default
     outs = []
-    for v in range(5):
+    for v in range(6):
         plan.variant = v
         assert plan.variant == v
         outs.append(plan.solve_source_host(f[1:-1, 1:-1]))
         assert_parity_2d(oracle, outs[-1], ref, TOL)
-    for v in range(1, 5):
+    for v in range(1, 6):
         assert rel_err(outs[v], outs[0]) < TOL  # same system, different rounding only
     v = plan.tune(4)
-    assert v in range(5)
+    assert v in range(6)
     assert np.array_equal(plan.solve_source_host(f[1:-1, 1:-1]), outs[v])
     with pytest.raises(hh.HHError):
-        plan.variant = 5
+        plan.variant = 6
     plan.close()
 
 
