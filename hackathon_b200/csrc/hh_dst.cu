@@ -425,18 +425,22 @@ template <int R> __device__ __forceinline__ void dft_r(double2 (&v)[R]) { DifRA<
 __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
 template <int M> struct WCfg;
-template <> struct WCfg<1024> { static constexpr int TL = 32, R = 32, WPC = 2; };
-template <> struct WCfg<512>  { static constexpr int TL = 16, R = 32, WPC = 2; };
-template <> struct WCfg<256>  { static constexpr int TL = 16, R = 16, WPC = 4; };
-template <> struct WCfg<128>  { static constexpr int TL = 8,  R = 16, WPC = 4; };
-template <> struct WCfg<64>   { static constexpr int TL = 8,  R = 8,  WPC = 4; };
+// TL lanes per line, R values per lane, WPC warps per CTA, NBUF line buffers per warp in the rows
+// kernel (2: the next line loads while one is transformed; 1: more warps per SM instead), MINB
+// CTAs per SM the register budget is sized for
+template <> struct WCfg<1024> { static constexpr int TL = 32, R = 32, WPC = 2, NBUF = 2, MINB = 3; };
+template <> struct WCfg<512>  { static constexpr int TL = 16, R = 32, WPC = 2, NBUF = 2, MINB = 3; };
+template <> struct WCfg<256>  { static constexpr int TL = 16, R = 16, WPC = 4, NBUF = 2, MINB = 3; };
+template <> struct WCfg<128>  { static constexpr int TL = 8,  R = 16, WPC = 4, NBUF = 2, MINB = 3; };
+template <> struct WCfg<64>   { static constexpr int TL = 8,  R = 8,  WPC = 4, NBUF = 2, MINB = 3; };
 
 template <int M> struct WGeom {
     static constexpr int TL = WCfg<M>::TL, R = WCfg<M>::R, WPC = WCfg<M>::WPC;
     static constexpr int LPW = 32 / TL, KB = M / (2 * TL);
     // one line's buffer: raw line, transpose [R][TL + 1], Y (k + k/KB), outputs ((2KB + 1) per 2KB)
     static constexpr int BUF = cmax(R * (TL + 1), cmax(M + M / KB, M + M / (2 * KB))) + 1;
-    static constexpr int WARP_ELEMS = 2 * LPW * BUF; // two buffer sets per warp
+    static constexpr int NBUF = WCfg<M>::NBUF;
+    static constexpr int WARP_ELEMS = NBUF * LPW * BUF; // NBUF buffer sets per warp
     static constexpr int SMEM = 16 * WPC + 16 * WARP_ELEMS * WPC;
 };
 
@@ -568,7 +572,7 @@ __device__ __forceinline__ void w_transform(XLoad xload, double2 *buf, int l, bo
 // ---- rows: lines g = 0 .. nlines*nplanes-1 at in + (g / nlines) in_plane + (g % nlines) in_ld
 // with x_1..x_N at offsets 0..N-1, likewise for the output; in and out may be the same buffer.
 template <int M>
-__global__ void __launch_bounds__(32 * WCfg<M>::WPC, 3)
+__global__ void __launch_bounds__(32 * WCfg<M>::WPC, WCfg<M>::MINB)
     k_dst1_w(const double2 *in, double2 *out, long nlines, long nplanes, long in_ld, long out_ld, long in_plane,
              long out_plane, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
     using G = WGeom<M>;
@@ -600,9 +604,10 @@ __global__ void __launch_bounds__(32 * WCfg<M>::WPC, 3)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncwarp();
+    constexpr int NBUF = G::NBUF;
     if (lane == 0) {
         fetch(g0, 0);
-        if (g0 + stride < groups) fetch(g0 + stride, 1);
+        if (NBUF == 2 && g0 + stride < groups) fetch(g0 + stride, 1);
     }
     WConst<M> K;
     K.load(l, tw, sn);
@@ -610,11 +615,11 @@ __global__ void __launch_bounds__(32 * WCfg<M>::WPC, 3)
     int  it = 0;
     long failed = -1;
     for (long grp = g0; grp < groups; grp += stride, it++) {
-        const int s = it & 1;
+        const int s = NBUF == 2 ? (it & 1) : 0;
         double2  *buf = sets + (s * LPW + c) * BUF;
         const long line = grp * LPW + c;
         const bool live = line < total;
-        if (!mbar_wait_parity(&bar[s], (it >> 1) & 1)) {
+        if (!mbar_wait_parity(&bar[s], NBUF == 2 ? (it >> 1) & 1 : it & 1)) {
             if (lane == 0) atomicExch(err, 1);
             failed = grp;
             break;
@@ -632,13 +637,17 @@ __global__ void __launch_bounds__(32 * WCfg<M>::WPC, 3)
         // generic-proxy accesses before the asynchronous copy that overwrites them)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncwarp();
-        if (lane == 0 && grp + 2 * stride < groups) fetch(grp + 2 * stride, s);
+        if (lane == 0 && grp + NBUF * stride < groups) fetch(grp + NBUF * stride, s);
     }
     // after an expired wait, give the copies still in flight a bounded chance to land before the
     // CTA's shared memory is released
     if (failed >= 0 && lane == 0) {
-        mbar_wait_parity(&bar[it & 1], (it >> 1) & 1);
-        if (failed + stride < groups) mbar_wait_parity(&bar[(it + 1) & 1], ((it + 1) >> 1) & 1);
+        if (NBUF == 1) {
+            mbar_wait_parity(&bar[0], it & 1);
+        } else {
+            mbar_wait_parity(&bar[it & 1], (it >> 1) & 1);
+            if (failed + stride < groups) mbar_wait_parity(&bar[(it + 1) & 1], ((it + 1) >> 1) & 1);
+        }
     }
 }
 

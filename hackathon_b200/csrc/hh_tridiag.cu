@@ -87,6 +87,9 @@ __device__ __forceinline__ double2 first_pivot(double2 dia) {
 
 // One thread per line: runs the Thomas recurrence over the whole line (the reference's LU(),
 // 2D LU.c:25-40 / 3D LU.c:51-72) and keeps 1/P of the row before each kSeg-row segment.
+// CONST_ROWS: the stencil rows are the same along the line, so they are formed once (the same
+// values the per-row evaluation gives) and the recurrence runs without memory traffic.
+template <bool CONST_ROWS>
 __global__ void k_factor(int lines, int rows, int prow, const double *__restrict__ mu,
                          const double2 *__restrict__ subt, const double2 *__restrict__ diagt,
                          const double2 *__restrict__ supt, double2 *__restrict__ Pv) {
@@ -95,19 +98,29 @@ __global__ void k_factor(int lines, int rows, int prow, const double *__restrict
     const double m0 = mu[q], m1 = mu[lines + q], m2 = mu[2 * lines + q];
     double2 ui = first_pivot(shifted(diagt, prow, 0, m0, m1, m2));
     double2 up_prev = shifted(supt, prow, 0, m0, m1, m2);
+    const double2 sub_c = shifted(subt, prow, 0, m0, m1, m2), dia_c = shifted(diagt, prow, 0, m0, m1, m2);
     Pv[q] = make_double2(0.0, 0.0);
     for (int r = 1; r < rows; r++) {
         if (r % kSeg == 0) Pv[(long)(r / kSeg) * lines + q] = ui;
         double2 L;
-        ui = factor_step(shifted(subt, prow, r, m0, m1, m2), shifted(diagt, prow, r, m0, m1, m2), up_prev, ui, L);
-        up_prev = shifted(supt, prow, r, m0, m1, m2);
+        if constexpr (CONST_ROWS) {
+            ui = factor_step(sub_c, dia_c, up_prev, ui, L);
+        } else {
+            ui = factor_step(shifted(subt, prow, r, m0, m1, m2), shifted(diagt, prow, r, m0, m1, m2), up_prev, ui,
+                             L);
+            up_prev = shifted(supt, prow, r, m0, m1, m2);
+        }
     }
 }
 
 int launch_factor(Plan *p, const double2 *subt, const double2 *diagt, const double2 *supt) {
-    const int nt = 128;
-    k_factor<<<(p->lines + nt - 1) / nt, nt, 0, p->ctx->stream>>>(p->lines, p->rows, p->prow, p->mu, subt, diagt,
-                                                                   supt, p->Pv);
+    const int nt = 64;
+    if (p->const_rows)
+        k_factor<true><<<(p->lines + nt - 1) / nt, nt, 0, p->ctx->stream>>>(p->lines, p->rows, p->prow, p->mu, subt,
+                                                                             diagt, supt, p->Pv);
+    else
+        k_factor<false><<<(p->lines + nt - 1) / nt, nt, 0, p->ctx->stream>>>(p->lines, p->rows, p->prow, p->mu, subt,
+                                                                              diagt, supt, p->Pv);
     HH_CUDA(cudaGetLastError());
     p->ctx->launches++;
     return HH_OK;
