@@ -643,6 +643,12 @@ __device__ __forceinline__ double lds_keep(const double *p) {
     return v;
 }
 
+// Order 6 with 16-row segments keeps the reciprocal pivots in shared memory, one column per
+// thread: in registers they would not fit beside the two solves' rows.
+template <int SRC, int KS> struct SymUIS {
+    static constexpr bool value = SRC == 6 && KS >= 16;
+};
+
 // Intra-warp inclusive scan of B over the segments of each line in the warp, with the stage
 // multipliers tab[j * NT] (the thread's own map product at stage j).  FWD composes left to right.
 template <int CW, bool FWD>
@@ -683,9 +689,9 @@ template <int SRC, int NT, int CW, bool TINT, int NR, int KS>
 __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double2 *__restrict__ out, int rows,
                                           long row_stride, long field, int b_begin, int b_end, long off0,
                                           bool live, int r0, int sl, int w, int c, const double2 (&Lr)[KS],
-                                          const double2 (&ui)[KS], double2 ui_in, double2 s, double2 c1, double c2,
-                                          double2 cT, SymSmem<NT / 32, CW, NR> &sm, double2 *pre,
-                                          const double2 *tabF, const double2 *tabB, const double *ttF,
+                                          const double2 (&ui)[KS], const double2 *uis, double2 ui_in, double2 s,
+                                          double2 c1, double c2, double2 cT, SymSmem<NT / 32, CW, NR> &sm,
+                                          double2 *pre, const double2 *tabF, const double2 *tabB, const double *ttF,
                                           const double *ttB, const SymParams &sp) {
     constexpr int NW = NT / 32, SPW = 32 / CW, LOG = ilog2_t<SPW>();
     constexpr int HALO = (SRC == 4 || SRC == 6) ? 1 : 0;
@@ -694,12 +700,19 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
     static_assert(CW * NR <= 128 && NT >= 256, "cross-warp thread ranges");
     const int     t = threadIdx.x;
     const double2 zero = make_double2(0.0, 0.0);
+    // reciprocal pivot of row r0 + k: in registers, or (order 6 with 16-row segments, where the
+    // two solves' rows fill the registers) in shared memory, one column per thread
+    constexpr bool UIS = SymUIS<SRC, KS>::value;
+    auto UI = [&](int k) -> double2 {
+        if constexpr (UIS) return lds_keep(uis + k * NT + t);
+        else return ui[k];
+    };
     // forward multiplier of row r0 + k: kept in registers, or (order 6, where registers are
     // short) re-formed from the reciprocal pivots as the set-up does
     constexpr bool KEEP_L = SRC != 6;
     auto LF = [&](int k) -> double2 {
         if constexpr (KEEP_L) return Lr[k];
-        return cmul(s, k == 0 ? ui_in : ui[k - 1]);
+        else return cmul(s, k == 0 ? ui_in : UI(k - 1));
     };
     // Pade factors of row r0 + k: the constants in warps whose rows all lie in [9, rows)
     auto PL = [&](int k) -> double {
@@ -843,7 +856,7 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
         for (int k = KS - 1; k >= 0; k--) {
 #pragma unroll
             for (int r = 0; r < NR; r++) {
-                xh[r] = cmul(ui[k], zfms(v[r][k], s, xh[r]));
+                xh[r] = cmul(UI(k), zfms(v[r][k], s, xh[r]));
                 if constexpr (SRC == 6)
                     wh[r] = make_double2(PU(k) * (g[r][k].x - wh[r].x), PU(k) * (g[r][k].y - wh[r].y));
             }
@@ -896,7 +909,7 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
             for (int k = KS - 1; k >= 0; k--) {
 #pragma unroll
                 for (int r = 0; r < NR; r++) {
-                    x[r] = cmul(ui[k], zfms(v[r][k], s, x[r]));
+                    x[r] = cmul(UI(k), zfms(v[r][k], s, x[r]));
                     v[r][k] = x[r];
                     if constexpr (SRC == 6) {
                         ww[r] = make_double2(PU(k) * (g[r][k].x - ww[r].x), PU(k) * (g[r][k].y - ww[r].y));
@@ -956,7 +969,9 @@ __global__ void __launch_bounds__(NT, MINB)
     double2 *pre = dyn;                                 // [NR][KS + 2][NT]
     double2 *tabF = pre + NR * (KS + 2) * NT;         // [LOG + 1][NT]
     double2 *tabB = tabF + (LOG + 1) * NT;              // [LOG + 1][NT]
-    double  *ttF = reinterpret_cast<double *>(tabB + (LOG + 1) * NT); // [LOG + 1][NT] (order 6)
+    constexpr bool UIS = SymUIS<SRC, KS>::value;
+    double2 *uis = tabB + (LOG + 1) * NT;               // [KS][NT] (UIS)
+    double  *ttF = reinterpret_cast<double *>(uis + (UIS ? KS * NT : 0)); // [LOG + 1][NT] (order 6)
     double  *ttB = ttF + (LOG + 1) * NT;
     (void)HALO;
 
@@ -986,6 +1001,7 @@ __global__ void __launch_bounds__(NT, MINB)
                 else ui[k] = factor_step(s, d, s, uprev, Lr[k]);
             }
             uprev = ui[k];
+            if constexpr (UIS) uis[k * NT + t] = ui[k];
             Af = cmul(Af, make_double2(-Lr[k].x, -Lr[k].y));
             const double2 tau = cmul(s, ui[k]);
             Ab = cmul(Ab, make_double2(-tau.x, -tau.y));
@@ -1053,10 +1069,10 @@ __global__ void __launch_bounds__(NT, MINB)
     const bool tint = (w * SPW * KS >= 9) && ((w + 1) * SPW * KS <= rows);
     if (SRC == 6 && tint)
         sym_chunk<SRC, NT, CW, true, NR, KS>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0, sl, w, c, Lr,
-                                     ui, ui_in, s, c1, c2, cT, sm, pre, tabF, tabB, ttF, ttB, sp);
+                                     ui, uis, ui_in, s, c1, c2, cT, sm, pre, tabF, tabB, ttF, ttB, sp);
     else
         sym_chunk<SRC, NT, CW, false, NR, KS>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0, sl, w, c, Lr,
-                                      ui, ui_in, s, c1, c2, cT, sm, pre, tabF, tabB, ttF, ttB, sp);
+                                      ui, uis, ui_in, s, c1, c2, cT, sm, pre, tabF, tabB, ttF, ttB, sp);
 }
 
 // Right-hand sides per CTA: the chunk whose grid has the smallest wave-quantised cost,
@@ -1086,7 +1102,8 @@ static int launch_sym_t(Plan *p, const double2 *in, double2 *out, int batch) {
     sp.uinf = p->pade_uinf;
     sp.pl = p->pade_l;
     sp.pu = p->pade_u;
-    const int shm = (int)(sizeof(double2) * (NR * (KS + 2) * NT + 2 * (LOG + 1) * NT) +
+    const int shm = (int)(sizeof(double2) * (NR * (KS + 2) * NT + 2 * (LOG + 1) * NT +
+                                             (SymUIS<SRC, KS>::value ? KS * NT : 0)) +
                           (SRC == 6 ? sizeof(double) * 2 * (LOG + 1) * NT : 0));
     HH_CUDA(cudaFuncSetAttribute(k_line_solve_sym<SRC, NT, CW, MINB, NR, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  shm));
@@ -1128,7 +1145,8 @@ bool sym_solve_supported(const Plan *p, int src_order) {
 
 // Variants of the symmetric kernel: 2 = two CTAs per SM, 3 = one CTA per SM (no register cap),
 // 4 = one CTA per SM with two right-hand sides per pass, 5 = one CTA per SM with 16-row segments
-// (twice the lines per CTA: wider contiguous row pieces in global memory, half the scans).
+// (twice the lines per CTA: wider contiguous row pieces in global memory, half the scans; at
+// order 6 the reciprocal pivots move to shared memory).
 template <int SRC> static int launch_sym_variant(Plan *p, const double2 *in, double2 *out, int batch) {
     switch (p->variant) {
     case 3: return launch_sym_src<SRC, 1, 1, kSeg>(p, in, out, batch);
