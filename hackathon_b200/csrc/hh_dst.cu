@@ -377,50 +377,52 @@ __device__ __forceinline__ constexpr double sinpi64(int m) {
 __device__ __forceinline__ constexpr double sin_m64(int m) { return m <= 32 ? sinpi64(m) : sinpi64(64 - m); }
 __device__ __forceinline__ constexpr double cos_m64(int m) { return m <= 32 ? sinpi64(32 - m) : -sinpi64(m - 32); }
 
-// v * exp(-2 pi i t / R), 0 <= t < R/2, R <= 64 (angle pi m / 64 with m = 128 t / R)
-template <int R, int t> __device__ __forceinline__ double2 twr_mul(double2 v) {
+// Radix-2 decimation-in-time butterfly with twiddle w = exp(-2 pi i t / R), R <= 64 (angle
+// pi m / 64, m = 128 t / R):  a <- a + w b,  b <- a - w b.  With a non-trivial twiddle the
+// difference takes four fused multiply-adds and the sum is 2a minus it, six operations in all.
+template <int R, int t> __device__ __forceinline__ void dit_bfly(double2 &a, double2 &b) {
     constexpr int m = t * (128 / R);
-    if constexpr (t == 0) return v;
-    else if constexpr (m == 32) return make_double2(v.y, -v.x);
-    else if constexpr (m == 16) {
-        constexpr double r = sinpi64(16);
-        return make_double2((v.x + v.y) * r, (v.y - v.x) * r);
-    } else if constexpr (m == 48) {
-        constexpr double r = sinpi64(16);
-        return make_double2((v.y - v.x) * r, -(v.x + v.y) * r);
+    const double2 x = a;
+    if constexpr (t == 0) {
+        a = cadd(x, b);
+        b = csub(x, b);
+    } else if constexpr (m == 32) { // w = -i, w b = (b.y, -b.x)
+        a = make_double2(x.x + b.y, x.y - b.x);
+        b = make_double2(x.x - b.y, x.y + b.x);
     } else {
-        constexpr double c = cos_m64(m), s = sin_m64(m);
-        return make_double2(fma(v.x, c, v.y * s), fma(v.y, c, -(v.x * s)));
+        constexpr double c = cos_m64(m), sn = sin_m64(m); // w = c - i sn, w b = (c b.x + sn b.y, c b.y - sn b.x)
+        const double2 d = make_double2(fma(-c, b.x, fma(-sn, b.y, x.x)), fma(-c, b.y, fma(sn, b.x, x.y)));
+        a = make_double2(fma(2.0, x.x, -d.x), fma(2.0, x.y, -d.y));
+        b = d;
     }
 }
-template <int R, int SPAN, int J> struct DifRB {
+template <int R, int SPAN, int J> struct DitB {
     __device__ __forceinline__ static void run(double2 (&v)[R], int start) {
         if constexpr (J < SPAN) {
-            const double2 a = v[start + J], b = v[start + J + SPAN];
-            v[start + J] = cadd(a, b);
-            v[start + J + SPAN] = twr_mul<R, J * (R / (2 * SPAN))>(csub(a, b));
-            DifRB<R, SPAN, J + 1>::run(v, start);
+            dit_bfly<R, J * (R / (2 * SPAN))>(v[start + J], v[start + J + SPAN]);
+            DitB<R, SPAN, J + 1>::run(v, start);
         }
     }
 };
-template <int R, int SPAN, int START> struct DifRS {
+template <int R, int SPAN, int START> struct DitS {
     __device__ __forceinline__ static void run(double2 (&v)[R]) {
         if constexpr (START < R) {
-            DifRB<R, SPAN, 0>::run(v, START);
-            DifRS<R, SPAN, START + 2 * SPAN>::run(v);
+            DitB<R, SPAN, 0>::run(v, START);
+            DitS<R, SPAN, START + 2 * SPAN>::run(v);
         }
     }
 };
-template <int R, int SPAN> struct DifRA {
+template <int R, int SPAN> struct DitA {
     __device__ __forceinline__ static void run(double2 (&v)[R]) {
-        if constexpr (SPAN >= 1) {
-            DifRS<R, SPAN, 0>::run(v);
-            DifRA<R, SPAN / 2>::run(v);
+        if constexpr (SPAN < R) {
+            DitS<R, SPAN, 0>::run(v);
+            DitA<R, SPAN * 2>::run(v);
         }
     }
 };
-// forward R-point DFT in registers (R <= 64); X[k] = v[bitrev(k)]
-template <int R> __device__ __forceinline__ void dft_r(double2 (&v)[R]) { DifRA<R, R / 2>::run(v); }
+// forward R-point DFT in registers (R <= 64) of x held in bit-reversed order, v[bitrev(q)] = x_q;
+// on return v[k] = X_k
+template <int R> __device__ __forceinline__ void dft_dit(double2 (&v)[R]) { DitA<R, 1>::run(v); }
 
 __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 
@@ -498,7 +500,8 @@ __device__ __forceinline__ void w_transform(XLoad xload, double2 *buf, int l, bo
     const double2 zero = make_double2(0.0, 0.0);
     K.launder();
 
-    // ---- y_j = sin(pi j/M)(x_j + x_{M-j}) + (x_j - x_{M-j})/2,  j = l + TL q
+    // ---- y_j = sin(pi j/M)(x_j + x_{M-j}) + (x_j - x_{M-j})/2 = (s + 1/2) x_j + (s - 1/2) x_{M-j},
+    //      j = l + TL q, stored at v[bitrev(q)] for the decimation-in-time DFT
     double2 v[R];
 #pragma unroll
     for (int q = 0; q < R; q++) {
@@ -508,37 +511,39 @@ __device__ __forceinline__ void w_transform(XLoad xload, double2 *buf, int l, bo
             a = xload(j);
             m = xload(M - j);
         }
-        const double s = fma(K.sb, cos_m64(q * (64 / R)), K.cb * sin_m64(q * (64 / R))); // sin(pi j / M)
-        v[q] = make_double2(fma(s, a.x + m.x, 0.5 * (a.x - m.x)), fma(s, a.y + m.y, 0.5 * (a.y - m.y)));
+        const double sp = fma(K.sb, cos_m64(q * (64 / R)), fma(K.cb, sin_m64(q * (64 / R)), 0.5)); // sin(pi j/M) + 1/2
+        const double sm = sp - 1.0;
+        v[bitrev_c<R>(q)] = make_double2(fma(sp, a.x, sm * m.x), fma(sp, a.y, sm * m.y));
     }
     __syncwarp(); // staged input consumed
 
     // ---- R-point DFTs over q, twiddle W_M^{l k1}, transpose [k1][l]
-    dft_r<R>(v);
+    dft_dit<R>(v);
 #pragma unroll
     for (int k1 = 0; k1 < R; k1++)
-        buf[k1 * (TL + 1) + l] = k1 ? cmul(v[bitrev_c<R>(k1)], cmul(K.twa[k1 & 7], K.twb[k1 >> 3])) : v[0];
+        buf[k1 * (TL + 1) + l] = k1 ? cmul(v[k1], cmul(K.twa[k1 & 7], K.twb[k1 >> 3])) : v[0];
     __syncwarp();
-    double2 w2[R / TL][TL]; // lane l takes k1 = l + TL i with all TL values of l'
+    double2 w2[R / TL][TL]; // lane l takes k1 = l + TL i with all TL values of l', in bit-reversed order
 #pragma unroll
     for (int i = 0; i < R / TL; i++)
 #pragma unroll
-        for (int lp = 0; lp < TL; lp++) w2[i][lp] = buf[(l + TL * i) * (TL + 1) + lp];
+        for (int lp = 0; lp < TL; lp++) w2[i][bitrev_c<TL>(lp)] = buf[(l + TL * i) * (TL + 1) + lp];
     __syncwarp();
 
-    // ---- TL-point DFTs over l': Y_{k1 + R k2} = w2[i][bitrev(k2)]
+    // ---- TL-point DFTs over l': Y_{k1 + R k2} = w2[i][k2]
 #pragma unroll
     for (int i = 0; i < R / TL; i++) {
-        dft_r<TL>(w2[i]);
+        dft_dit<TL>(w2[i]);
 #pragma unroll
         for (int k2 = 0; k2 < TL; k2++) {
             const int k = l + TL * i + R * k2;
-            buf[k + k / KB] = w2[i][bitrev_c<TL>(k2)];
+            buf[k + k / KB] = w2[i][k2];
         }
     }
     __syncwarp();
 
-    // ---- post-processing on blocks k = KB l + u
+    // ---- post-processing on blocks k = KB l + u (the halves of (Y_k + Y_{M-k})/2 and
+    //      (Y_{M-k} - Y_k)/(2i) are folded into the output scale)
     double2 cs[KB], ev[KB];
     double2 run = zero;
 #pragma unroll
@@ -546,19 +551,19 @@ __device__ __forceinline__ void w_transform(XLoad xload, double2 *buf, int l, bo
         const int     k = KB * l + u;
         const double2 yk = buf[k + k / KB];
         if (k == 0) {
-            cs[u] = make_double2(0.5 * yk.x, 0.5 * yk.y);
+            cs[u] = yk;
             ev[u] = zero;
         } else {
             const int     km = M - k;
             const double2 ym = buf[km + km / KB];
-            cs[u] = make_double2(0.5 * (yk.x + ym.x), 0.5 * (yk.y + ym.y));
-            ev[u] = make_double2(0.5 * (ym.y - yk.y), -0.5 * (ym.x - yk.x)); // (Y_{M-k} - Y_k)/(2i)
+            cs[u] = cadd(yk, ym);
+            ev[u] = make_double2(ym.y - yk.y, yk.x - ym.x); // (Y_{M-k} - Y_k)/i
         }
         run = cadd(run, cs[u]);
         cs[u] = run;
     }
     const double2 pre = csub(line_scan<TL, LPW, INTER>(run, l), run);
-    const double  coef = sqrt(2.0 / M);
+    const double  coef = 0.5 * sqrt(2.0 / M);
     __syncwarp(); // every read of Y is done
 #pragma unroll
     for (int u = 0; u < KB; u++) {
