@@ -714,6 +714,12 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
         if constexpr (KEEP_L) return Lr[k];
         else return cmul(s, k == 0 ? ui_in : UI(k - 1));
     };
+    // backward multiplier of row r0 + k, tau_k = s ui_k (= L_{k+1} where that row exists)
+    const double2 tau_last = KEEP_L ? cmul(s, ui[KS - 1]) : s;
+    auto TAU = [&](int k) -> double2 {
+        if constexpr (KEEP_L) return k + 1 < KS ? Lr[k + 1] : tau_last;
+        else return cmul(s, UI(k));
+    };
     // Pade factors of row r0 + k: the constants in warps whose rows all lie in [9, rows)
     auto PL = [&](int k) -> double {
         if constexpr (TINT) return sp.linf;
@@ -833,13 +839,17 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
                 z[r] = zero;
                 if constexpr (SRC == 6) z[r] = zaxpy(bfe[r], aeF, sm.eF[r][w][c]);
             }
+            // the rows keep ui_k y_k, so that the back substitution is x_k = ui_k y_k - tau_k x_{k+1}
+            double2 up = ui_in;
 #pragma unroll
             for (int k = 0; k < KS; k++) {
-                const double2 l = LF(k);
+                const double2 u = UI(k);
+                const double2 l = KEEP_L ? Lr[k] : cmul(s, up);
+                up = u;
 #pragma unroll
                 for (int r = 0; r < NR; r++) {
                     y[r] = zfms(v[r][k], l, y[r]);
-                    v[r][k] = y[r];
+                    v[r][k] = cmul(u, y[r]);
                     if constexpr (SRC == 6) {
                         z[r] = make_double2(fma(-PL(k), z[r].x, g[r][k].x), fma(-PL(k), z[r].y, g[r][k].y));
                         g[r][k] = z[r];
@@ -848,7 +858,7 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
             }
         }
 
-        // ---- back substitution x_r = ui_r (y_r - s x_{r+1});  Pade: w_r = pu_r (z_r - w_{r+1})
+        // ---- back substitution x_r = ui_r y_r - tau_r x_{r+1};  Pade: w_r = pu_r (z_r - w_{r+1})
         double2 xh[NR], wh[NR];
 #pragma unroll
         for (int r = 0; r < NR; r++) { xh[r] = zero; wh[r] = zero; }
@@ -856,7 +866,7 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
         for (int k = KS - 1; k >= 0; k--) {
 #pragma unroll
             for (int r = 0; r < NR; r++) {
-                xh[r] = cmul(UI(k), zfms(v[r][k], s, xh[r]));
+                xh[r] = zfms(v[r][k], TAU(k), xh[r]);
                 if constexpr (SRC == 6)
                     wh[r] = make_double2(PU(k) * (g[r][k].x - wh[r].x), PU(k) * (g[r][k].y - wh[r].y));
             }
@@ -909,7 +919,7 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
             for (int k = KS - 1; k >= 0; k--) {
 #pragma unroll
                 for (int r = 0; r < NR; r++) {
-                    x[r] = cmul(UI(k), zfms(v[r][k], s, x[r]));
+                    x[r] = zfms(v[r][k], TAU(k), x[r]);
                     v[r][k] = x[r];
                     if constexpr (SRC == 6) {
                         ww[r] = make_double2(PU(k) * (g[r][k].x - ww[r].x), PU(k) * (g[r][k].y - ww[r].y));
