@@ -677,19 +677,6 @@ template <int M> struct WColGeom {
     static_assert(NBOX == 1 || (LPW * BR) % 8 == 0, "box offsets must stay 128-byte aligned");
 };
 
-__device__ __forceinline__ void tma_tile_load(void *dst, const CUtensorMap *map, int x, int j, int p, uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(
-            smem_u32(dst)),
-        "l"(map), "r"(0), "r"(x), "r"(j), "r"(p), "r"(smem_u32(bar))
-        : "memory");
-}
-__device__ __forceinline__ void tma_tile_store(const CUtensorMap *map, int x, int j, int p, const void *src) {
-    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(map),
-                 "r"(0), "r"(x), "r"(j), "r"(p), "r"(smem_u32(src))
-                 : "memory");
-}
-
 template <int M>
 __global__ void __launch_bounds__(32 * WCfg<M>::WPC, 3)
     k_dst1_wc(const __grid_constant__ CUtensorMap in_map, const __grid_constant__ CUtensorMap out_map, long ncols,

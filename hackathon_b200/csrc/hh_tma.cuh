@@ -76,6 +76,19 @@ __device__ __forceinline__ void tma_store_5d(const CUtensorMap *map, int c1, int
                  "r"(0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(src))
                  : "memory");
 }
+// 4-D tensor copies over (re/im, x, j, plane) maps: one box at column x, row j, plane p
+__device__ __forceinline__ void tma_tile_load(void *dst, const CUtensorMap *map, int x, int j, int p, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(
+            smem_u32(dst)),
+        "l"(map), "r"(0), "r"(x), "r"(j), "r"(p), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_tile_store(const CUtensorMap *map, int x, int j, int p, const void *src) {
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(map),
+                 "r"(0), "r"(x), "r"(j), "r"(p), "r"(smem_u32(src))
+                 : "memory");
+}
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }

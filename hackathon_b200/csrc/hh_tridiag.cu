@@ -50,6 +50,7 @@
 // It is applied in registers before the Helmholtz solve, so the RHS assembly costs no extra
 // HBM traffic.
 #include "hh_internal.cuh"
+#include "hh_tma.cuh"
 
 #include <algorithm>
 
@@ -522,7 +523,7 @@ int padded_rows(int rows) {
     return best;
 }
 
-int solve_variant_count() { return kNumVariants + 4; }
+int solve_variant_count() { return kNumVariants + 5; }
 
 template <int SRC, bool CR, int NT, int MINB>
 static int launch_solve_t(Plan *p, const double2 *in, double2 *out, int batch) {
@@ -619,6 +620,7 @@ __device__ __forceinline__ double2 zaxpy(double2 a, double b, double2 c) { // a 
 template <int NT> __host__ __device__ constexpr int ilog2_t() { return NT <= 1 ? 0 : 1 + ilog2_t<NT / 2>(); }
 
 template <int NW, int CW, int NR> struct SymSmem {
+    uint64_t tbar[2];                 // completion of the tile copies (TMA-tile input)
     double2 AwF[NW][CW], AwB[NW][CW]; // warp totals of the segment multipliers (main solve)
     double  awF[NW][CW], awB[NW][CW]; // the same for the Pade solve (real multipliers)
     double2 BwF[NR][NW][CW], BwB[NR][NW][CW]; // warp totals of the B values, per right-hand side
@@ -682,20 +684,39 @@ struct SymParams {
     const double *pl, *pu; // Pade factors (rows >= 9 equal linf, uinf)
 };
 
+// TMA-tile input of the symmetric line solve: one right-hand side of the CTA's CW lines arrives
+// as a tile [rows][CW] in shared memory, brought by tensor copies over a (re/im, line, row,
+// right-hand side) map in boxes of br rows, NBUF right-hand sides ahead.  Thread 0 issues the
+// copies; the outputs are stored from registers as in the per-thread prefetch form.
+template <int SRC> struct SymTileBufs {
+    static constexpr int value = SRC == 6 ? 1 : 2; // order 6 spends the space on its pivots
+};
+
+struct SymTio {
+    const CUtensorMap *in_map;
+    double2           *tin;  // NBUF tiles of `tile` elements
+    uint64_t          *bar;  // one per tile
+    int               *err;
+    int                x0, br, nbox, tile;
+    unsigned           tile_bytes;
+};
+
 // One chunk of right-hand sides for the thread's segment, NR of them side by side (independent
 // dependency chains, shared barriers).  TINT = the warp's rows all lie in [9, rows) (constant
 // Pade factors).
-template <int SRC, int NT, int CW, bool TINT, int NR, int KS>
+template <int SRC, int NT, int CW, bool TINT, int NR, int KS, bool TIO>
 __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double2 *__restrict__ out, int rows,
                                           long row_stride, long field, int b_begin, int b_end, long off0,
                                           bool live, int r0, int sl, int w, int c, const double2 (&Lr)[KS],
                                           const double2 (&ui)[KS], const double2 *uis, double2 ui_in, double2 s,
                                           double2 c1, double c2, double2 cT, SymSmem<NT / 32, CW, NR> &sm,
                                           double2 *pre, const double2 *tabF, const double2 *tabB, const double *ttF,
-                                          const double *ttB, const SymParams &sp) {
+                                          const double *ttB, const SymParams &sp, const SymTio &tio) {
     constexpr int NW = NT / 32, SPW = 32 / CW, LOG = ilog2_t<SPW>();
     constexpr int HALO = (SRC == 4 || SRC == 6) ? 1 : 0;
     constexpr int SLOTS = KS + 2;
+    constexpr int  NBUF = SymTileBufs<SRC>::value;
+    static_assert(!TIO || NR == 1, "tile I/O moves one right-hand side at a time");
     // cross-warp sequential passes: main solve on threads [0, CW NR), Pade solve on [128, 128 + CW NR)
     static_assert(CW * NR <= 128 && NT >= 256, "cross-warp thread ranges");
     const int     t = threadIdx.x;
@@ -732,6 +753,13 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
         return r < 9 ? sm.pu[r] : (r < rows ? sp.uinf : 0.0);
     };
 
+    // the tile copies of right-hand side b into tile buffer u, issued by thread 0
+    auto tile_load = [&](int b, int u) {
+        double2 *dst = tio.tin + (long)u * tio.tile;
+        mbar_expect_tx(tio.bar + u, tio.tile_bytes);
+        for (int x = 0; x < tio.nbox; x++)
+            tma_tile_load(dst + (long)x * tio.br * CW, tio.in_map, tio.x0, x * tio.br, b, tio.bar + u);
+    };
     auto prefetch = [&](int b) {
 #pragma unroll
         for (int r = 0; r < NR; r++) {
@@ -745,22 +773,35 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
         }
         cp_async_commit();
     };
-    prefetch(b_begin);
-    for (int b = b_begin; b < b_end; b += NR) {
+    if constexpr (!TIO) prefetch(b_begin); // with tile I/O the first tile was requested at kernel start
+    int it = 0;
+    for (int b = b_begin; b < b_end; b += NR, it++) {
         double2 v[NR][KS], g[NR][KS], gm[NR], gp[NR];
-        cp_async_wait_all();
+        bool    landed = true;
+        if constexpr (TIO) {
+            const int u = NBUF == 2 ? (it & 1) : 0;
+            landed = mbar_wait_parity(tio.bar + u, NBUF == 2 ? (it >> 1) & 1 : it & 1);
+            const double2 *tl = tio.tin + (long)u * tio.tile + c;
 #pragma unroll
-        for (int r = 0; r < NR; r++) {
+            for (int k = 0; k < KS; k++) v[0][k] = (r0 + k < rows) ? tl[(r0 + k) * CW] : zero;
+            gm[0] = (HALO && r0 > 0) ? tl[(r0 - 1) * CW] : zero;
+            gp[0] = (HALO && r0 + KS < rows) ? tl[(r0 + KS) * CW] : zero;
+            fence_async_smem(); // these reads before the copy that refills the tile
+        } else {
+            cp_async_wait_all();
 #pragma unroll
-            for (int k = 0; k < KS; k++) v[r][k] = pre[(r * SLOTS + k + 1) * NT + t];
-            gm[r] = zero;
-            gp[r] = zero;
-            if constexpr (HALO) {
-                gm[r] = pre[(r * SLOTS) * NT + t];
-                gp[r] = pre[(r * SLOTS + KS + 1) * NT + t];
+            for (int r = 0; r < NR; r++) {
+#pragma unroll
+                for (int k = 0; k < KS; k++) v[r][k] = pre[(r * SLOTS + k + 1) * NT + t];
+                gm[r] = zero;
+                gp[r] = zero;
+                if constexpr (HALO) {
+                    gm[r] = pre[(r * SLOTS) * NT + t];
+                    gp[r] = pre[(r * SLOTS + KS + 1) * NT + t];
+                }
             }
+            if (b + NR < b_end) prefetch(b + NR);
         }
-        if (b + NR < b_end) prefetch(b + NR);
 
         // ---- compact right-hand side (order 6: the A^-1 part; g keeps the source for T^-1)
 #pragma unroll
@@ -809,7 +850,23 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
             }
             if (sl == 0) { Bfe[r] = zero; bfe[r] = zero; }
         }
-        __syncthreads();
+        if constexpr (TIO) {
+            if (__syncthreads_or(!landed)) { // a tile copy did not land: report and leave together
+                if (t == 0) {
+                    atomicExch(tio.err, 1);
+                    // copies still in flight get a bounded chance to land before the memory is released
+                    for (int j = 0; j < NBUF && b + j < b_end; j++) {
+                        const int jt = it + j;
+                        mbar_wait_parity(tio.bar + (NBUF == 2 ? (jt & 1) : 0), NBUF == 2 ? (jt >> 1) & 1 : jt & 1);
+                    }
+                }
+                return;
+            }
+            // every thread has read this tile: it takes the right-hand side NBUF ahead
+            if (t == 0 && b + NBUF < b_end) tile_load(b + NBUF, NBUF == 2 ? (it & 1) : 0);
+        } else {
+            __syncthreads();
+        }
         if (t < CW * NR) {
             const int r = t / CW, cc = t % CW;
             double2   E = zero;
@@ -967,17 +1024,29 @@ __device__ __forceinline__ M sym_scan_table(M a, M *tab, int NT_, int sl, M one)
     return a;
 }
 
-template <int SRC, int NT, int CW, int MINB, int NR, int KS>
+// Elements of one TMA tile [rows][cw] (whole 128-byte units), and the rows per box.
+__host__ __device__ inline int sym_tile_rows_per_box(int rows) { return rows < 256 ? rows : 256; }
+__host__ __device__ inline int sym_tile_elems(int rows, int cw) {
+    const int br = sym_tile_rows_per_box(rows), nbox = (rows + br - 1) / br;
+    return (nbox * br * cw + 7) / 8 * 8;
+}
+
+template <int SRC, int NT, int CW, int MINB, int NR, int KS, bool TIO>
 __global__ void __launch_bounds__(NT, MINB)
     k_line_solve_sym(const double2 *__restrict__ in, double2 *__restrict__ out, int lines, int rows, long row_stride,
                      long field, int batch, int rb, const double2 *__restrict__ Pv, const double2 *__restrict__ subt,
-                     const double2 *__restrict__ diagt, int prow, const double *__restrict__ mu, SymParams sp) {
+                     const double2 *__restrict__ diagt, int prow, const double *__restrict__ mu, SymParams sp,
+                     const __grid_constant__ CUtensorMap in_map, int *err) {
     constexpr int NW = NT / 32, SPW = 32 / CW, LOG = ilog2_t<SPW>();
     constexpr int HALO = (SRC == 4 || SRC == 6) ? 1 : 0;
     __shared__ SymSmem<NW, CW, NR> sm;
-    extern __shared__ double2 dyn[];
-    double2 *pre = dyn;                                 // [NR][KS + 2][NT]
-    double2 *tabF = pre + NR * (KS + 2) * NT;         // [LOG + 1][NT]
+    extern __shared__ __align__(128) unsigned char dyn_raw[];
+    // 128-byte aligned start (tensor copies need it; the allocation carries 128 bytes of slack)
+    double2 *dyn = reinterpret_cast<double2 *>(dyn_raw + ((128u - (smem_u32(dyn_raw) & 127u)) & 127u));
+    // per-thread prefetch slots [NR][KS + 2][NT], or the input tiles
+    const int io_elems = TIO ? sym_tile_elems(rows, CW) * SymTileBufs<SRC>::value : NR * (KS + 2) * NT;
+    double2  *pre = dyn;
+    double2 *tabF = pre + io_elems;                     // [LOG + 1][NT]
     double2 *tabB = tabF + (LOG + 1) * NT;              // [LOG + 1][NT]
     constexpr bool UIS = SymUIS<SRC, KS>::value;
     double2 *uis = tabB + (LOG + 1) * NT;               // [KS][NT] (UIS)
@@ -988,6 +1057,30 @@ __global__ void __launch_bounds__(NT, MINB)
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const int c = t % CW, seg = t / CW, sl = lane / CW;
     const int q = blockIdx.x * CW + c;
+    SymTio    tio{};
+    if constexpr (TIO) {
+        constexpr int NBUF = SymTileBufs<SRC>::value;
+        tio.in_map = &in_map;
+        tio.tin = pre;
+        tio.bar = sm.tbar;
+        tio.err = err;
+        tio.x0 = blockIdx.x * CW;
+        tio.br = sym_tile_rows_per_box(rows);
+        tio.nbox = (rows + tio.br - 1) / tio.br;
+        tio.tile = sym_tile_elems(rows, CW);
+        tio.tile_bytes = (unsigned)(tio.nbox * tio.br * CW * 16);
+        if (t == 0) { // the first right-hand sides' tiles come in while the factors are set up
+            const int b0 = blockIdx.y * rb, b1 = min(batch, b0 + rb);
+            for (int u = 0; u < NBUF; u++) mbar_init(tio.bar + u, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            for (int u = 0; u < NBUF && b0 + u < b1; u++) {
+                double2 *dst = tio.tin + (long)u * tio.tile;
+                mbar_expect_tx(tio.bar + u, tio.tile_bytes);
+                for (int x = 0; x < tio.nbox; x++)
+                    tma_tile_load(dst + (long)x * tio.br * CW, tio.in_map, tio.x0, x * tio.br, b0 + u, tio.bar + u);
+            }
+        }
+    }
     const bool live = q < lines;
     const int  qq = live ? q : 0;
     const int  r0 = seg * KS;
@@ -1078,11 +1171,13 @@ __global__ void __launch_bounds__(NT, MINB)
     // warps whose rows all lie in [9, rows) use the constant Pade factors
     const bool tint = (w * SPW * KS >= 9) && ((w + 1) * SPW * KS <= rows);
     if (SRC == 6 && tint)
-        sym_chunk<SRC, NT, CW, true, NR, KS>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0, sl, w, c, Lr,
-                                     ui, uis, ui_in, s, c1, c2, cT, sm, pre, tabF, tabB, ttF, ttB, sp);
+        sym_chunk<SRC, NT, CW, true, NR, KS, TIO>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0, sl,
+                                                  w, c, Lr, ui, uis, ui_in, s, c1, c2, cT, sm, pre, tabF, tabB, ttF,
+                                                  ttB, sp, tio);
     else
-        sym_chunk<SRC, NT, CW, false, NR, KS>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0, sl, w, c, Lr,
-                                      ui, uis, ui_in, s, c1, c2, cT, sm, pre, tabF, tabB, ttF, ttB, sp);
+        sym_chunk<SRC, NT, CW, false, NR, KS, TIO>(in, out, rows, row_stride, field, b_begin, b_end, off0, live, r0,
+                                                   sl, w, c, Lr, ui, uis, ui_in, s, c1, c2, cT, sm, pre, tabF, tabB,
+                                                   ttF, ttB, sp, tio);
 }
 
 // Right-hand sides per CTA: the chunk whose grid has the smallest wave-quantised cost,
@@ -1101,7 +1196,18 @@ static int pick_rb(long groups, int batch, int resident, int nr) {
     return best;
 }
 
-template <int SRC, int CW, int MINB, int NR, int KS>
+// (re/im, line, row, right-hand side) map of a batch of line-solve fields, boxes of cw lines by
+// br rows
+static int encode_line_map(CUtensorMap *map, const double2 *base, const Plan *p, int batch, int cw, int br) {
+    const unsigned long long dims[4] = {2, (unsigned long long)p->lines, (unsigned long long)p->rows,
+                                        (unsigned long long)batch};
+    const unsigned long long strides[3] = {16, (unsigned long long)p->row_stride * 16,
+                                           (unsigned long long)p->field * 16};
+    const unsigned           box[4] = {2, (unsigned)cw, (unsigned)br, 1};
+    return encode_tensor_map(map, base, 4, dims, strides, box);
+}
+
+template <int SRC, int CW, int MINB, int NR, int KS, bool TIO>
 static int launch_sym_t(Plan *p, const double2 *in, double2 *out, int batch) {
     constexpr int NT = 256, SPW = 32 / CW, LOG = ilog2_t<SPW>();
     SymParams sp;
@@ -1112,56 +1218,65 @@ static int launch_sym_t(Plan *p, const double2 *in, double2 *out, int batch) {
     sp.uinf = p->pade_uinf;
     sp.pl = p->pade_l;
     sp.pu = p->pade_u;
-    const int shm = (int)(sizeof(double2) * (NR * (KS + 2) * NT + 2 * (LOG + 1) * NT +
-                                             (SymUIS<SRC, KS>::value ? KS * NT : 0)) +
-                          (SRC == 6 ? sizeof(double) * 2 * (LOG + 1) * NT : 0));
-    HH_CUDA(cudaFuncSetAttribute(k_line_solve_sym<SRC, NT, CW, MINB, NR, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const int io_elems = TIO ? sym_tile_elems(p->rows, CW) * SymTileBufs<SRC>::value : NR * (KS + 2) * NT;
+    const int shm = 128 + (int)(sizeof(double2) * (io_elems + 2 * (LOG + 1) * NT +
+                                                   (SymUIS<SRC, KS>::value ? KS * NT : 0)) +
+                                (SRC == 6 ? sizeof(double) * 2 * (LOG + 1) * NT : 0));
+    CUtensorMap in_map{};
+    if constexpr (TIO) HH_TRY(encode_line_map(&in_map, in, p, batch, CW, sym_tile_rows_per_box(p->rows)));
+    HH_CUDA(cudaFuncSetAttribute(k_line_solve_sym<SRC, NT, CW, MINB, NR, KS, TIO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  shm));
     const long groups = (p->lines + CW - 1) / CW;
     int blocks_per_sm = 0, dev = 0, sms = 148;
-    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_line_solve_sym<SRC, NT, CW, MINB, NR, KS>, NT,
+    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_line_solve_sym<SRC, NT, CW, MINB, NR, KS, TIO>, NT,
                                                           shm));
     HH_CUDA(cudaGetDevice(&dev));
     HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int rb = pick_rb(groups, batch, std::max(1, blocks_per_sm) * sms, NR);
     const int chunks = (batch + rb - 1) / rb;
     dim3 grid((unsigned)groups, (unsigned)chunks);
-    k_line_solve_sym<SRC, NT, CW, MINB, NR, KS><<<grid, NT, shm, p->ctx->stream>>>(
-        in, out, p->lines, p->rows, p->row_stride, p->field, batch, rb, p->Pv, p->subt, p->diagt, p->prow, p->mu, sp);
+    k_line_solve_sym<SRC, NT, CW, MINB, NR, KS, TIO><<<grid, NT, shm, p->ctx->stream>>>(
+        in, out, p->lines, p->rows, p->row_stride, p->field, batch, rb, p->Pv, p->subt, p->diagt, p->prow, p->mu, sp,
+        in_map, p->ctx->err_word);
     HH_CUDA(cudaGetLastError());
     p->ctx->launches++;
     return HH_OK;
 }
 
-template <int SRC, int MINB, int NR, int KS> static int launch_sym_src(Plan *p, const double2 *in, double2 *out, int batch) {
+// TIO: tile I/O where a line group is at least four lines (64-byte row pieces); narrower groups
+// keep the per-thread prefetch.
+template <int SRC, int MINB, int NR, int KS, bool TIO = false>
+static int launch_sym_src(Plan *p, const double2 *in, double2 *out, int batch) {
     // segments per line: a power of two P >= rows / KS with 8 <= P <= 256 (CW = 256 / P lines per CTA)
     int P = 8;
     while (P * KS < p->rows) P <<= 1;
     switch (P) {
-    case 8: return launch_sym_t<SRC, 32, MINB, 1, KS>(p, in, out, batch); // per-RHS scan arrays would not fit
-    case 16: return launch_sym_t<SRC, 16, MINB, NR, KS>(p, in, out, batch);
-    case 32: return launch_sym_t<SRC, 8, MINB, NR, KS>(p, in, out, batch);
-    case 64: return launch_sym_t<SRC, 4, MINB, NR, KS>(p, in, out, batch);
-    case 128: return launch_sym_t<SRC, 2, MINB, NR, KS>(p, in, out, batch);
-    case 256: return launch_sym_t<SRC, 1, MINB, NR, KS>(p, in, out, batch);
+    case 8: return launch_sym_t<SRC, 32, MINB, 1, KS, TIO>(p, in, out, batch); // per-RHS scan arrays would not fit
+    case 16: return launch_sym_t<SRC, 16, MINB, NR, KS, TIO>(p, in, out, batch);
+    case 32: return launch_sym_t<SRC, 8, MINB, NR, KS, TIO>(p, in, out, batch);
+    case 64: return launch_sym_t<SRC, 4, MINB, NR, KS, TIO>(p, in, out, batch);
+    case 128: return launch_sym_t<SRC, 2, MINB, NR, KS, false>(p, in, out, batch);
+    case 256: return launch_sym_t<SRC, 1, MINB, NR, KS, false>(p, in, out, batch);
     default: set_error("symmetric line solve: %d rows", p->rows); return HH_ERR_UNSUPPORTED;
     }
 }
 
 bool sym_solve_supported(const Plan *p, int src_order) {
-    const int max_rows = 256 * (p->variant == 5 ? 16 : kSeg);
+    const int max_rows = 256 * (p->variant >= 5 ? 16 : kSeg);
     return p->sym && p->rows <= max_rows && (src_order != 6 || (p->pf_ok && p->pade_l));
 }
 
 // Variants of the symmetric kernel: 2 = two CTAs per SM, 3 = one CTA per SM (no register cap),
 // 4 = one CTA per SM with two right-hand sides per pass, 5 = one CTA per SM with 16-row segments
 // (twice the lines per CTA: wider contiguous row pieces in global memory, half the scans; at
-// order 6 the reciprocal pivots move to shared memory).
+// order 6 the reciprocal pivots move to shared memory), 6 = variant 5 with each right-hand side
+// brought in as a TMA tile where a CTA holds at least four lines.
 template <int SRC> static int launch_sym_variant(Plan *p, const double2 *in, double2 *out, int batch) {
     switch (p->variant) {
     case 3: return launch_sym_src<SRC, 1, 1, kSeg>(p, in, out, batch);
     case 4: return launch_sym_src<SRC, 1, 2, kSeg>(p, in, out, batch);
     case 5: return launch_sym_src<SRC, 1, 1, 16>(p, in, out, batch);
+    case 6: return launch_sym_src<SRC, 1, 1, 16, true>(p, in, out, batch);
     default: return launch_sym_src<SRC, 2, 1, kSeg>(p, in, out, batch);
     }
 }

@@ -108,9 +108,10 @@ long hh_plan_field_size(const hh_plan *plan);  /* complex values per right-hand 
 
 /* The line solve has several kernels: 0 and 1 for any stencil (512 threads x 1 block or 256 x 2
  * per SM); for constant-coefficient symmetric lines (the Helmholtz plans) also 2 (two blocks
- * per SM), 3 (one block, no register cap), 4 (two right-hand sides per pass) and 5 (16-row
- * segments).  hh_plan_tune times each on `batch` right-hand sides and keeps the fastest
- * (blocking; not during stream capture); set/get select one directly. */
+ * per SM), 3 (one block, no register cap), 4 (two right-hand sides per pass), 5 (16-row
+ * segments) and 6 (16-row segments, right-hand sides brought in as TMA tiles).  hh_plan_tune
+ * times each on `batch` right-hand sides and keeps the fastest (blocking; not during stream
+ * capture); set/get select one directly. */
 int hh_plan_tune(hh_plan *plan, int batch);
 int hh_plan_set_variant(hh_plan *plan, int variant);
 int hh_plan_variant(const hh_plan *plan);

@@ -69,26 +69,28 @@ def test_batch_equals_single(ctx, oracle):
 @pytest.mark.parametrize("n,order,k", [(15, 6, 10.0), (31, 6, 10.0), (63, 2, 30.0), (255, 4, 50.0), (511, 6, 20.0),
                                        (1023, 6, 50.0), (1023, 4, 10.0), (2047, 6, 100.0)])
 def test_every_line_solve_variant_matches_oracle(ctx, oracle, n, order, k):
-    """Each line-solve kernel on its own (0/1: general rows, 512 or 256 threads; 2..5: symmetric
+    """Each line-solve kernel on its own (0/1: general rows, 512 or 256 threads; 2..6: symmetric
     constant rows with the order-6 partial fractions -- 2 or 1 blocks per SM, one or two
-    right-hand sides per pass, 8- or 16-row segments), then hh_plan_tune's choice."""
+    right-hand sides per pass, 8- or 16-row segments, right-hand sides moved as TMA tiles), then
+    hh_plan_tune's choice."""
     f = _source(n, 7 * n + order)
     ref = oracle.pipeline_2d(n, order, k, f)
     plan = hh.Plan.helmholtz(ctx, 2, n, order, k)
     assert plan.variant == 2  # constant k: the symmetric kernel by default
     outs = []
-    for v in range(6):
+    for v in range(7):
         plan.variant = v
         assert plan.variant == v
         outs.append(plan.solve_source_host(f[1:-1, 1:-1]))
         assert_parity_2d(oracle, outs[-1], ref, TOL)
-    for v in range(1, 6):
+    for v in range(1, 7):
         assert rel_err(outs[v], outs[0]) < TOL  # same system, different rounding only
+    assert np.array_equal(outs[6], outs[5])  # tile I/O moves the same values as variant 5
     v = plan.tune(4)
-    assert v in range(6)
+    assert v in range(7)
     assert np.array_equal(plan.solve_source_host(f[1:-1, 1:-1]), outs[v])
     with pytest.raises(hh.HHError):
-        plan.variant = 6
+        plan.variant = 7
     plan.close()
 
 
@@ -117,6 +119,30 @@ def test_host_path_chunked_equals_device_path(ctx):
     plan.solve_source(f, u, B)
     ctx.synchronize()
     assert np.array_equal(host, u.cpu().numpy())
+    plan.close()
+
+
+@pytest.mark.parametrize("dim,n,order,batch", [(2, 1023, 4, 7), (2, 1023, 6, 5), (2, 511, 2, 9), (2, 127, 4, 3),
+                                               (3, 63, 6, 3), (3, 127, 4, 2)])
+def test_tile_io_variant_equals_prefetch_variant(ctx, dim, n, order, batch):
+    """Variant 6 moves each right-hand side as TMA tiles (loads, and outside order 6 stores);
+    on device buffers of several right-hand sides, over every chunk boundary of the grid, its
+    result is bitwise variant 5's, whose arithmetic it shares."""
+    torch = pytest.importorskip("torch")
+    g = torch.Generator().manual_seed(1000 * dim + n + order)
+    shape = (batch,) + (n,) * dim
+    f = torch.complex(torch.randn(shape, generator=g, dtype=torch.float64),
+                      torch.randn(shape, generator=g, dtype=torch.float64)).cuda()
+    plan = hh.Plan.helmholtz(ctx, dim, n, order, 40.0)
+    outs = []
+    for v in (5, 6):
+        plan.variant = v
+        u = torch.full_like(f, float("nan"))
+        plan.solve_source(f, u, batch)
+        ctx.synchronize()
+        outs.append(u.cpu())
+    assert torch.isfinite(outs[1]).all()
+    assert torch.equal(outs[0], outs[1])
     plan.close()
 
 
