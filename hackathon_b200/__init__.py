@@ -68,6 +68,8 @@ SIGNATURES = {
     "hh_solve_source": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source_host": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source_host_noalloc": (_i, [_vp, _vp, _vp, _i]),
+    "hh_residual": (_i, [_vp, _vp, _vp, _vp, _i, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "hh_solve_refined": (_i, [_vp, _vp, _vp, _i, C.c_double, _i, C.POINTER(_i), C.POINTER(C.c_double)]),
     "hh_coefficients2d": (_i, [_i, _i, _d, _d, C.POINTER(_vp)]),
     "hh_coefficients3d": (_i, [_i, _i, _d, _d, C.POINTER(_vp)]),
     "hh_ctx_set_stage_timing": (_i, [_vp, _i]),
@@ -243,6 +245,23 @@ class Plan:
 
     def solve_source(self, f, u, batch: int = 1):
         check(lib().hh_solve_source(self.h, _addr(f), _addr(u), batch), "hh_solve_source")
+
+    def solve_refined(self, rhs, sol, batch: int = 1, tol: float = 1e-10, max_iter: int = 10):
+        """hh_solve_refined on device buffers; returns (corrections, relative residual)."""
+        it, rr = C.c_int(), C.c_double()
+        check(lib().hh_solve_refined(self.h, _addr(rhs), _addr(sol), batch, tol, max_iter, C.byref(it), C.byref(rr)),
+              "hh_solve_refined")
+        return it.value, rr.value
+
+    def residual(self, sol, rhs, res, batch: int = 1, norms: bool = False):
+        """hh_residual on device buffers: res = A_h sol - rhs; with norms, (max|res|, max|rhs|)."""
+        if not norms:
+            check(lib().hh_residual(self.h, _addr(sol), _addr(rhs), _addr(res), batch, None, None), "hh_residual")
+            return None
+        mr, mf = C.c_double(), C.c_double()
+        check(lib().hh_residual(self.h, _addr(sol), _addr(rhs), _addr(res), batch, C.byref(mr), C.byref(mf)),
+              "hh_residual")
+        return mr.value, mf.value
 
     # -- host numpy arrays
     def solve_host(self, rhs: np.ndarray) -> np.ndarray:

@@ -124,6 +124,8 @@ extern "C" int hh_ctx_destroy(hh_ctx *x) {
     for (auto &kv : x->c.sn) cudaFree(kv.second);
     for (auto &kv : x->c.dense) cudaFree(kv.second);
     cudaFree(x->c.err_word);
+    cudaFree(x->c.norms);
+    cudaFree(x->c.refine_work);
     cudaFree(x->stage);
     for (cudaEvent_t e : x->c.chunk_ev) cudaEventDestroy(e);
     if (x->c.copy_in) cudaStreamDestroy(x->c.copy_in);
@@ -581,27 +583,28 @@ extern "C" int hh_plan_tune(hh_plan *pl, int batch) {
 }
 
 // -------------------------------------------------------------------- solve ------
-static int transform_forward(Plan &p, const double2 *in, double2 *out, int batch) {
+// lp: single-precision transform arithmetic (the refined solve's low-precision solves)
+static int transform_forward(Plan &p, const double2 *in, double2 *out, int batch, bool lp = false) {
     Ctx *c = p.ctx;
-    if (p.dim == 2) return launch_dst_rows(c, p.nx, (long)p.ny * batch, in, p.nx, out, p.nx);
+    if (p.dim == 2) return launch_dst_rows(c, p.nx, (long)p.ny * batch, in, p.nx, out, p.nx, lp);
     const long plane = (long)p.nx * p.ny, planes = (long)p.nz * batch;
-    HH_TRY(launch_dst_rows(c, p.nx, (long)p.ny * planes, in, p.nx, out, p.nx));
+    HH_TRY(launch_dst_rows(c, p.nx, (long)p.ny * planes, in, p.nx, out, p.nx, lp));
     for (long p0 = 0; p0 < planes; p0 += 65535) {
         const long np = (planes - p0 < 65535) ? planes - p0 : 65535;
-        HH_TRY(launch_dst_cols(c, p.ny, p.nx, np, out + p0 * plane, p.nx, plane, out + p0 * plane));
+        HH_TRY(launch_dst_cols(c, p.ny, p.nx, np, out + p0 * plane, p.nx, plane, out + p0 * plane, lp));
     }
     return HH_OK;
 }
 
-static int transform_inverse(Plan &p, double2 *buf, int batch) {
+static int transform_inverse(Plan &p, double2 *buf, int batch, bool lp = false) {
     Ctx *c = p.ctx;
-    if (p.dim == 2) return launch_dst_rows(c, p.nx, (long)p.ny * batch, buf, p.nx, buf, p.nx);
+    if (p.dim == 2) return launch_dst_rows(c, p.nx, (long)p.ny * batch, buf, p.nx, buf, p.nx, lp);
     const long plane = (long)p.nx * p.ny, planes = (long)p.nz * batch;
     for (long p0 = 0; p0 < planes; p0 += 65535) {
         const long np = (planes - p0 < 65535) ? planes - p0 : 65535;
-        HH_TRY(launch_dst_cols(c, p.ny, p.nx, np, buf + p0 * plane, p.nx, plane, buf + p0 * plane));
+        HH_TRY(launch_dst_cols(c, p.ny, p.nx, np, buf + p0 * plane, p.nx, plane, buf + p0 * plane, lp));
     }
-    return launch_dst_rows(c, p.nx, (long)p.ny * planes, buf, p.nx, buf, p.nx);
+    return launch_dst_rows(c, p.nx, (long)p.ny * planes, buf, p.nx, buf, p.nx, lp);
 }
 
 static int check_batch(hh_plan *pl, int batch) {
@@ -626,6 +629,95 @@ extern "C" int hh_solve(hh_plan *pl, const double *rhs, double *sol, int batch) 
     HH_TRY(stage_mark(*p.ctx, 2));
     HH_TRY(transform_inverse(p, u, batch));
     return stage_mark(*p.ctx, 3);
+}
+
+// The residual maxima buffer of a context (two words, made on first use).
+static int ctx_norms(Ctx *c, unsigned long long **out) {
+    if (!c->norms) HH_CUDA(cudaMalloc(&c->norms, 2 * sizeof(unsigned long long)));
+    *out = c->norms;
+    return HH_OK;
+}
+
+extern "C" int hh_residual(hh_plan *pl, const double *sol, const double *rhs, double *res, int batch,
+                           double *max_res, double *max_rhs) {
+    HH_TRY(check_batch(pl, batch));
+    if (batch == 0) return HH_OK;
+    if (!sol || !rhs || !res) { set_error("hh_residual: null buffer"); return HH_ERR_INVALID; }
+    if (res == sol) { set_error("hh_residual: res must not be the solution buffer"); return HH_ERR_INVALID; }
+    Plan &p = pl->p;
+    Ctx  *c = p.ctx;
+    HH_CUDA(cudaSetDevice(c->device));
+    unsigned long long *norms = nullptr;
+    const bool          want = max_res || max_rhs;
+    if (want) {
+        HH_TRY(ctx_norms(c, &norms));
+        HH_CUDA(cudaMemsetAsync(norms, 0, 2 * sizeof(unsigned long long), c->stream));
+    }
+    HH_TRY(launch_residual(&p, (const double2 *)sol, (const double2 *)rhs, (double2 *)res, batch, norms));
+    if (want) {
+        unsigned long long h[2];
+        HH_CUDA(cudaMemcpyAsync(h, norms, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+        HH_CUDA(cudaStreamSynchronize(c->stream));
+        double v[2];
+        memcpy(v, h, sizeof(v));
+        if (max_res) *max_res = v[0];
+        if (max_rhs) *max_rhs = v[1];
+    }
+    return HH_OK;
+}
+
+// Mixed-precision refined solve of assembled right-hand sides: each solve of the loop runs its
+// transforms in single-precision arithmetic and its line solves in FP64; the residual and the
+// update are FP64.  u_0 = S(rhs); u_{k+1} = u_k - S(A_h u_k - rhs) until max|A_h u - rhs| /
+// max|rhs| <= tol or max_iter corrections.
+extern "C" int hh_solve_refined(hh_plan *pl, const double *rhs, double *sol, int batch, double tol, int max_iter,
+                                int *iters, double *rel_res) {
+    HH_TRY(check_batch(pl, batch));
+    if (batch == 0) return HH_OK;
+    if (!rhs || !sol) { set_error("hh_solve_refined: null buffer"); return HH_ERR_INVALID; }
+    if (rhs == sol) { set_error("hh_solve_refined: rhs and sol must be different buffers"); return HH_ERR_INVALID; }
+    if (!(tol > 0.0) || max_iter < 0) { set_error("hh_solve_refined: tol must be > 0, max_iter >= 0"); return HH_ERR_INVALID; }
+    Plan &p = pl->p;
+    Ctx  *c = p.ctx;
+    HH_CUDA(cudaSetDevice(c->device));
+    const long need = p.field * (long)batch;
+    if (c->refine_elems < need) { // the workspace grows to the largest batch seen
+        HH_CUDA(cudaStreamSynchronize(c->stream));
+        cudaFree(c->refine_work);
+        c->refine_work = nullptr;
+        c->refine_elems = 0;
+        HH_CUDA(cudaMalloc(&c->refine_work, sizeof(double2) * (size_t)need));
+        c->refine_elems = need;
+    }
+    unsigned long long *norms = nullptr;
+    HH_TRY(ctx_norms(c, &norms));
+    double2       *u = (double2 *)sol, *w = c->refine_work;
+    const double2 *f = (const double2 *)rhs;
+    auto low_solve = [&](const double2 *in, double2 *out) -> int {
+        HH_TRY(transform_forward(p, in, out, batch, true));
+        HH_TRY(launch_line_solve(&p, out, out, batch, 0));
+        return transform_inverse(p, out, batch, true);
+    };
+    HH_TRY(low_solve(f, u));
+    int    k = 0;
+    double rr = 0.0;
+    for (;;) {
+        HH_CUDA(cudaMemsetAsync(norms, 0, 2 * sizeof(unsigned long long), c->stream));
+        HH_TRY(launch_residual(&p, u, f, w, batch, norms));
+        unsigned long long h[2];
+        HH_CUDA(cudaMemcpyAsync(h, norms, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+        HH_CUDA(cudaStreamSynchronize(c->stream));
+        double v[2];
+        memcpy(v, h, sizeof(v));
+        rr = v[1] > 0.0 ? v[0] / v[1] : 0.0;
+        if (rr <= tol || k >= max_iter) break;
+        HH_TRY(low_solve(w, w));
+        HH_TRY(launch_axpy(c, u, w, -1.0, need));
+        k++;
+    }
+    if (iters) *iters = k;
+    if (rel_res) *rel_res = rr;
+    return hh_ctx_synchronize(reinterpret_cast<hh_ctx *>(c)); // kernel-reported failures
 }
 
 extern "C" int hh_solve_source(hh_plan *pl, const double *f, double *u, int batch) {

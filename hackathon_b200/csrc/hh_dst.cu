@@ -574,9 +574,159 @@ __device__ __forceinline__ void w_transform(XLoad xload, double2 *buf, int l, bo
     __syncwarp();
 }
 
+// ---- single-precision arithmetic form of w_transform (the refined solve's correction
+// transforms): the same algorithm and data movement, float arithmetic, FP64 in and out.  The
+// staged line and the results stay double2 in shared memory; the exchanges in between are
+// float2 in the same buffer.
+__device__ __forceinline__ float2 fadd2(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 fsub2(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+template <int R, int t> __device__ __forceinline__ void dit_bfly_f(float2 &a, float2 &b) {
+    constexpr int m = t * (128 / R);
+    const float2  x = a;
+    if constexpr (t == 0) {
+        a = fadd2(x, b);
+        b = fsub2(x, b);
+    } else if constexpr (m == 32) {
+        a = make_float2(x.x + b.y, x.y - b.x);
+        b = make_float2(x.x - b.y, x.y + b.x);
+    } else {
+        constexpr float c = (float)cos_m64(m), sn = (float)sin_m64(m);
+        const float2    d = make_float2(fmaf(-c, b.x, fmaf(-sn, b.y, x.x)), fmaf(-c, b.y, fmaf(sn, b.x, x.y)));
+        a = make_float2(fmaf(2.0f, x.x, -d.x), fmaf(2.0f, x.y, -d.y));
+        b = d;
+    }
+}
+template <int R, int SPAN, int J> struct DitBF {
+    __device__ __forceinline__ static void run(float2 (&v)[R], int start) {
+        if constexpr (J < SPAN) {
+            dit_bfly_f<R, J * (R / (2 * SPAN))>(v[start + J], v[start + J + SPAN]);
+            DitBF<R, SPAN, J + 1>::run(v, start);
+        }
+    }
+};
+template <int R, int SPAN, int START> struct DitSF {
+    __device__ __forceinline__ static void run(float2 (&v)[R]) {
+        if constexpr (START < R) {
+            DitBF<R, SPAN, 0>::run(v, START);
+            DitSF<R, SPAN, START + 2 * SPAN>::run(v);
+        }
+    }
+};
+template <int R, int SPAN> struct DitAF {
+    __device__ __forceinline__ static void run(float2 (&v)[R]) {
+        if constexpr (SPAN < R) {
+            DitSF<R, SPAN, 0>::run(v);
+            DitAF<R, SPAN * 2>::run(v);
+        }
+    }
+};
+template <int R> __device__ __forceinline__ void dft_dit_f(float2 (&v)[R]) { DitAF<R, 1>::run(v); }
+
+template <int TL, int LPW, bool INTER> __device__ __forceinline__ float2 line_scan_f(float2 x, int l) {
+#pragma unroll
+    for (int off = 1; off < TL; off <<= 1) {
+        float ox, oy;
+        if constexpr (INTER) {
+            ox = __shfl_up_sync(0xffffffffu, x.x, off * LPW);
+            oy = __shfl_up_sync(0xffffffffu, x.y, off * LPW);
+        } else {
+            ox = __shfl_up_sync(0xffffffffu, x.x, off, TL);
+            oy = __shfl_up_sync(0xffffffffu, x.y, off, TL);
+        }
+        if (l >= off) { x.x += ox; x.y += oy; }
+    }
+    return x;
+}
+
+template <int M, bool INTER, typename XLoad>
+__device__ __forceinline__ void w_transform_lp(XLoad xload, double2 *buf, int l, bool live, WConst<M> &K) {
+    using G = WGeom<M>;
+    constexpr int TL = G::TL, R = G::R, LPW = G::LPW, KB = G::KB, K2 = 2 * KB;
+    constexpr int NB = WConst<M>::NB;
+    const float2  zero = make_float2(0.f, 0.f);
+    float2       *fb = reinterpret_cast<float2 *>(buf);
+    K.launder();
+    const float sb = (float)K.sb, cb = (float)K.cb;
+    float2      twa[8], twb[NB];
+#pragma unroll
+    for (int a = 0; a < 8; a++) twa[a] = make_float2((float)K.twa[a].x, (float)K.twa[a].y);
+#pragma unroll
+    for (int b = 0; b < NB; b++) twb[b] = make_float2((float)K.twb[b].x, (float)K.twb[b].y);
+
+    float2 v[R];
+#pragma unroll
+    for (int q = 0; q < R; q++) {
+        const int j = l + TL * q;
+        double2   a = make_double2(0.0, 0.0), m = a;
+        if (live && (q > 0 || l > 0)) {
+            a = xload(j);
+            m = xload(M - j);
+        }
+        const float sp = fmaf(sb, (float)cos_m64(q * (64 / R)), fmaf(cb, (float)sin_m64(q * (64 / R)), 0.5f));
+        const float sm = sp - 1.0f;
+        v[bitrev_c<R>(q)] = make_float2(fmaf(sp, (float)a.x, sm * (float)m.x), fmaf(sp, (float)a.y, sm * (float)m.y));
+    }
+    __syncwarp();
+
+    dft_dit_f<R>(v);
+#pragma unroll
+    for (int k1 = 0; k1 < R; k1++)
+        fb[k1 * (TL + 1) + l] = k1 ? fmul2(v[k1], fmul2(twa[k1 & 7], twb[k1 >> 3])) : v[0];
+    __syncwarp();
+    float2 w2[R / TL][TL];
+#pragma unroll
+    for (int i = 0; i < R / TL; i++)
+#pragma unroll
+        for (int lp = 0; lp < TL; lp++) w2[i][bitrev_c<TL>(lp)] = fb[(l + TL * i) * (TL + 1) + lp];
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < R / TL; i++) {
+        dft_dit_f<TL>(w2[i]);
+#pragma unroll
+        for (int k2 = 0; k2 < TL; k2++) {
+            const int k = l + TL * i + R * k2;
+            fb[k + k / KB] = w2[i][k2];
+        }
+    }
+    __syncwarp();
+
+    float2 cs[KB], ev[KB];
+    float2 run = zero;
+#pragma unroll
+    for (int u = 0; u < KB; u++) {
+        const int    k = KB * l + u;
+        const float2 yk = fb[k + k / KB];
+        if (k == 0) {
+            cs[u] = yk;
+            ev[u] = zero;
+        } else {
+            const int    km = M - k;
+            const float2 ym = fb[km + km / KB];
+            cs[u] = fadd2(yk, ym);
+            ev[u] = make_float2(ym.y - yk.y, yk.x - ym.x);
+        }
+        run = fadd2(run, cs[u]);
+        cs[u] = run;
+    }
+    const float2 pre = fsub2(line_scan_f<TL, LPW, INTER>(run, l), run);
+    const float  coef = (float)(0.5 * sqrt(2.0 / M));
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < KB; u++) {
+        const int    k = KB * l + u, po = 2 * k, pe = 2 * k - 1;
+        const float2 o = fadd2(pre, cs[u]);
+        buf[(K2 + 1) * (po / K2) + po % K2] = make_double2((double)(o.x * coef), (double)(o.y * coef));
+        if (k > 0) buf[(K2 + 1) * (pe / K2) + pe % K2] = make_double2((double)(ev[u].x * coef), (double)(ev[u].y * coef));
+    }
+    __syncwarp();
+}
+
 // ---- rows: lines g = 0 .. nlines*nplanes-1 at in + (g / nlines) in_plane + (g % nlines) in_ld
 // with x_1..x_N at offsets 0..N-1, likewise for the output; in and out may be the same buffer.
-template <int M>
+template <int M, bool LP = false>
 __global__ void __launch_bounds__(32 * WCfg<M>::WPC, WCfg<M>::MINB)
     k_dst1_w(const double2 *in, double2 *out, long nlines, long nplanes, long in_ld, long out_ld, long in_plane,
              long out_plane, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
@@ -629,7 +779,8 @@ __global__ void __launch_bounds__(32 * WCfg<M>::WPC, WCfg<M>::MINB)
             failed = grp;
             break;
         }
-        w_transform<M, false>([&](int j) { return buf[j - 1]; }, buf, l, live, K);
+        if constexpr (LP) w_transform_lp<M, false>([&](int j) { return buf[j - 1]; }, buf, l, live, K);
+        else w_transform<M, false>([&](int j) { return buf[j - 1]; }, buf, l, live, K);
         if (live) {
             double2 *dst = dst_of(line);
 #pragma unroll
@@ -677,7 +828,7 @@ template <int M> struct WColGeom {
     static_assert(NBOX == 1 || (LPW * BR) % 8 == 0, "box offsets must stay 128-byte aligned");
 };
 
-template <int M>
+template <int M, bool LP = false>
 __global__ void __launch_bounds__(32 * WCfg<M>::WPC, 3)
     k_dst1_wc(const __grid_constant__ CUtensorMap in_map, const __grid_constant__ CUtensorMap out_map, long ncols,
               long nplanes, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
@@ -734,7 +885,8 @@ __global__ void __launch_bounds__(32 * WCfg<M>::WPC, 3)
             failed = grp;
             break;
         }
-        w_transform<M, true>([&](int j) { return tile[(j - 1) * LPW + c]; }, xbuf, l, live, K);
+        if constexpr (LP) w_transform_lp<M, true>([&](int j) { return tile[(j - 1) * LPW + c]; }, xbuf, l, live, K);
+        else w_transform<M, true>([&](int j) { return tile[(j - 1) * LPW + c]; }, xbuf, l, live, K);
         // outputs into the tile ([j][c], rows past N untouched), then one tensor store per box
 #pragma unroll
         for (int q = 0; q < M / TL; q++) {
@@ -884,26 +1036,28 @@ template <int M, bool IS, bool OS> static int launch_fft(Ctx *c, const DstArgs &
     return HH_OK;
 }
 
-template <int M> static int launch_w(Ctx *c, const DstArgs &a) {
+template <int M, bool LP> static int launch_w(Ctx *c, const DstArgs &a) {
     using G = WGeom<M>;
     const double2 *tw;
     const double  *sn;
     HH_TRY(tables_for(c, M, &tw, &sn));
-    HH_CUDA(cudaFuncSetAttribute(k_dst1_w<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
+    HH_CUDA(cudaFuncSetAttribute(k_dst1_w<M, LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
     int dev = 0, sms = 148, per_sm = 0;
     HH_CUDA(cudaGetDevice(&dev));
     HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dst1_w<M>, 32 * G::WPC, G::SMEM));
+    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dst1_w<M, LP>, 32 * G::WPC, G::SMEM));
     const long groups = (a.nlines * a.planes + G::LPW - 1) / G::LPW;
     const long ctas = std::min<long>((groups + G::WPC - 1) / G::WPC, (long)std::max(1, per_sm) * sms);
-    k_dst1_w<M><<<(unsigned)ctas, 32 * G::WPC, G::SMEM, c->stream>>>(a.in, a.out, a.nlines, a.planes, a.in_ld, a.out_ld,
+    k_dst1_w<M, LP><<<(unsigned)ctas, 32 * G::WPC, G::SMEM, c->stream>>>(a.in, a.out, a.nlines, a.planes, a.in_ld, a.out_ld,
                                                                      a.in_plane, a.out_plane, tw, sn, c->err_word);
     HH_CUDA(cudaGetLastError());
     c->launches++;
     return HH_OK;
 }
 
-template <bool IS, bool OS> static int launch_dispatch(Ctx *c, int n, const DstArgs &a) {
+// LP: single-precision arithmetic where the persistent-warp kernels serve (n + 1 = 64 .. 1024);
+// the other kernels compute in FP64 either way.
+template <bool IS, bool OS, bool LP = false> static int launch_dispatch(Ctx *c, int n, const DstArgs &a) {
     if (n < 1) { set_error("DST length must be >= 1 (got %d)", n); return HH_ERR_INVALID; }
     if (a.nlines <= 0 || a.planes <= 0) return HH_OK;
     if (a.planes > 65535) { set_error("DST: too many planes (%ld)", a.planes); return HH_ERR_INVALID; }
@@ -913,11 +1067,11 @@ template <bool IS, bool OS> static int launch_dispatch(Ctx *c, int n, const DstA
     }
     if (!IS && !OS) {
         switch (n + 1) { // contiguous rows: persistent-warp kernels
-        case 64: return launch_w<64>(c, a);
-        case 128: return launch_w<128>(c, a);
-        case 256: return launch_w<256>(c, a);
-        case 512: return launch_w<512>(c, a);
-        case 1024: return launch_w<1024>(c, a);
+        case 64: return launch_w<64, LP>(c, a);
+        case 128: return launch_w<128, LP>(c, a);
+        case 256: return launch_w<256, LP>(c, a);
+        case 512: return launch_w<512, LP>(c, a);
+        case 1024: return launch_w<1024, LP>(c, a);
         default: break;
         }
     }
@@ -953,9 +1107,9 @@ template <bool IS, bool OS> static int launch_dispatch(Ctx *c, int n, const DstA
     return HH_OK;
 }
 
-int launch_dst_rows(Ctx *c, int n, long rows, const double2 *in, long in_ld, double2 *out, long out_ld) {
+int launch_dst_rows(Ctx *c, int n, long rows, const double2 *in, long in_ld, double2 *out, long out_ld, bool lp) {
     DstArgs a{in, out, rows, 1, in_ld, out_ld, 0, 0};
-    return launch_dispatch<false, false>(c, n, a);
+    return lp ? launch_dispatch<false, false, true>(c, n, a) : launch_dispatch<false, false>(c, n, a);
 }
 
 // 4-D tensor map over (re/im, column x, row j, plane) of complex doubles, boxes of `box_cols`
@@ -1000,7 +1154,8 @@ int encode_tensor_map(CUtensorMap *map, const void *base, int rank, const unsign
 }
 
 template <int M>
-static int launch_wc(Ctx *c, long ncols, long planes, const double2 *in, long ld, long plane_stride, double2 *out) {
+static int launch_wc(Ctx *c, long ncols, long planes, const double2 *in, long ld, long plane_stride, double2 *out,
+                     bool lp) {
     using G = WGeom<M>;
     using CG = WColGeom<M>;
     const double2 *tw;
@@ -1009,31 +1164,31 @@ static int launch_wc(Ctx *c, long ncols, long planes, const double2 *in, long ld
     CUtensorMap in_map, out_map;
     HH_TRY(encode_col_map(&in_map, in, ncols, M - 1, planes, ld, plane_stride, G::LPW, CG::BR));
     HH_TRY(encode_col_map(&out_map, out, ncols, M - 1, planes, ld, plane_stride, G::LPW, CG::BR));
-    HH_CUDA(cudaFuncSetAttribute(k_dst1_wc<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, CG::SMEM));
+    auto kern = lp ? k_dst1_wc<M, true> : k_dst1_wc<M, false>;
+    HH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, CG::SMEM));
     int dev = 0, sms = 148, per_sm = 0;
     HH_CUDA(cudaGetDevice(&dev));
     HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dst1_wc<M>, 32 * G::WPC, CG::SMEM));
+    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * G::WPC, CG::SMEM));
     const long groups = (ncols + G::LPW - 1) / G::LPW * planes;
     const long ctas = std::min<long>((groups + G::WPC - 1) / G::WPC, (long)std::max(1, per_sm) * sms);
-    k_dst1_wc<M><<<(unsigned)ctas, 32 * G::WPC, CG::SMEM, c->stream>>>(in_map, out_map, ncols, planes, tw, sn,
-                                                                       c->err_word);
+    kern<<<(unsigned)ctas, 32 * G::WPC, CG::SMEM, c->stream>>>(in_map, out_map, ncols, planes, tw, sn, c->err_word);
     HH_CUDA(cudaGetLastError());
     c->launches++;
     return HH_OK;
 }
 
 int launch_dst_cols(Ctx *c, int n, long ncols, long planes, const double2 *in, long ld, long plane_stride,
-                    double2 *out) {
+                    double2 *out, bool lp) {
     // tensor maps need 16-byte aligned bases (always true for double2) and byte strides below 2^40
     // (the tensor-map box never exceeds the tensor: at least LPW columns)
     if (planes > 0 && ld * 16 < (1L << 40) && plane_stride * 16 < (1L << 40) && planes < (1L << 31)) {
         switch (n + 1) {
-        case 64: if (ncols >= WGeom<64>::LPW) return launch_wc<64>(c, ncols, planes, in, ld, plane_stride, out); break;
-        case 128: if (ncols >= WGeom<128>::LPW) return launch_wc<128>(c, ncols, planes, in, ld, plane_stride, out); break;
-        case 256: if (ncols >= WGeom<256>::LPW) return launch_wc<256>(c, ncols, planes, in, ld, plane_stride, out); break;
-        case 512: if (ncols >= WGeom<512>::LPW) return launch_wc<512>(c, ncols, planes, in, ld, plane_stride, out); break;
-        case 1024: if (ncols >= WGeom<1024>::LPW) return launch_wc<1024>(c, ncols, planes, in, ld, plane_stride, out); break;
+        case 64: if (ncols >= WGeom<64>::LPW) return launch_wc<64>(c, ncols, planes, in, ld, plane_stride, out, lp); break;
+        case 128: if (ncols >= WGeom<128>::LPW) return launch_wc<128>(c, ncols, planes, in, ld, plane_stride, out, lp); break;
+        case 256: if (ncols >= WGeom<256>::LPW) return launch_wc<256>(c, ncols, planes, in, ld, plane_stride, out, lp); break;
+        case 512: if (ncols >= WGeom<512>::LPW) return launch_wc<512>(c, ncols, planes, in, ld, plane_stride, out, lp); break;
+        case 1024: if (ncols >= WGeom<1024>::LPW) return launch_wc<1024>(c, ncols, planes, in, ld, plane_stride, out, lp); break;
         default: break;
         }
     }

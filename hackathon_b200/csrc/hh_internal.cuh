@@ -83,6 +83,11 @@ struct Ctx {
     // plan memory pool (set by the request loop; null = cudaMalloc/cudaFree, synchronous set-up)
     cudaMemPool_t            pool = nullptr;
     std::vector<cudaEvent_t> chunk_ev;
+    // residual maxima (max |res|, max |rhs| as double bit patterns) and the refined form's
+    // workspace (one residual / correction field per right-hand side), made on first use
+    unsigned long long      *norms = nullptr;
+    double2                 *refine_work = nullptr;
+    long                     refine_elems = 0;
 };
 
 int tables_for(Ctx *c, int m, const double2 **tw, const double **sn);
@@ -120,11 +125,19 @@ struct Plan {
     double2  k2 = {0.0, 0.0};
 };
 
-int launch_dst_rows(Ctx *c, int n, long rows, const double2 *in, long in_ld, double2 *out, long out_ld);
+// lp: single-precision arithmetic (the refined solve's corrections) where the persistent-warp
+// kernels serve (n + 1 = 64 .. 1024); FP64 otherwise
+int launch_dst_rows(Ctx *c, int n, long rows, const double2 *in, long in_ld, double2 *out, long out_ld,
+                    bool lp = false);
 int launch_dst_cols(Ctx *c, int n, long ncols, long planes, const double2 *in, long ld, long plane_stride,
-                    double2 *out);
+                    double2 *out, bool lp = false);
 int launch_factor(Plan *p, const double2 *subt, const double2 *diagt, const double2 *supt);
 int launch_line_solve(Plan *p, const double2 *in, double2 *out, int batch, int src_order);
+// res = A_h u - rhs (FP64, zero Dirichlet ring); norms (optional, zeroed by the caller) receive
+// max |res| and max |rhs| over the batch as double bit patterns
+int launch_residual(Plan *p, const double2 *u, const double2 *rhs, double2 *res, int batch,
+                    unsigned long long *norms);
+int launch_axpy(Ctx *c, double2 *u, const double2 *v, double s, long n); // u += s v
 int read_device_error(Ctx *c, int *val);
 int segment_count(int rows);
 int padded_rows(int rows);

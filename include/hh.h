@@ -136,6 +136,26 @@ int hh_solve_source_host(hh_plan *plan, const double *f_host, double *u_host, in
  * contexts on a device: calls that overlap in time race and must be serialized by the caller. */
 int hh_solve_source_host_noalloc(hh_plan *plan, const double *f_host, double *u_host, int batch);
 
+/* FP64 residual res = A_h sol - rhs of the plan's compact operator for `batch` fields on the
+ * device, with a zero Dirichlet ring (the reference's residual(), 2D_Program/main_functions/
+ * residual.c:3-34, 3D_Program/main_functions/residual.c:42-96; its error-vs-analytic part is the
+ * caller's).  res must not be the sol buffer.  If max_res or max_rhs is not NULL the call waits
+ * and returns max |res| and max |rhs| over the batch (complex modulus). */
+int hh_residual(hh_plan *plan, const double *sol_dev, const double *rhs_dev, double *res_dev, int batch,
+                double *max_res, double *max_rhs);
+
+/* Mixed-precision refined solve of `batch` assembled right-hand sides on the device (the
+ * refined form of the survey's plan; the reference solves in plain FP64 only): every solve in
+ * the loop runs its DSTs in single-precision arithmetic (where n + 1 is a power of two up to
+ * 1024; FP64 otherwise) and its line solves in FP64, and hh_residual's FP64 residual drives
+ * the corrections:  u_0 = S(rhs),  u_{k+1} = u_k - S(A_h u_k - rhs)  until
+ * max|A_h u - rhs| / max|rhs| <= tol or max_iter corrections.  *iters and *rel_res (optional)
+ * receive the corrections made and the final relative residual; a result above tol is not an
+ * error.  Uses a context workspace of batch fields (allocated on first use, grown as needed).
+ * Blocking.  rhs and sol must be different buffers. */
+int hh_solve_refined(hh_plan *plan, const double *rhs_dev, double *sol_dev, int batch, double tol, int max_iter,
+                     int *iters, double *rel_res);
+
 /* Stencil coefficients the Helmholtz plans use (host arrays of n complex values each):
  * 2D order in bp,ap,b,a,bm,am order; 3D in a..dm order (12 arrays). */
 int hh_coefficients2d(int n, int order, double k_re, double k_im, double *const out[6]);
