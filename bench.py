@@ -234,6 +234,61 @@ def secondary_configs(hh, ctx, st, torch) -> dict:
     return out
 
 
+def refined_configs(hh, ctx, st, torch) -> dict:
+    """The mixed-precision refined form against the plain FP64 form on the same assembled
+    right-hand sides (seeded sine-mode fields used directly as the assembled rhs): 2D N=1023
+    order 6 k=50 batch 64, 2D N=2047 order 6 batch 16 with k in {10, 100, 400}, 3D N=255 order 6
+    k=30 batch 4.  Refinement to max|A_h u - rhs| / max|rhs| <= 1e-10.  The refined solve is
+    blocking (one residual read-back per correction), so both forms are timed with CUDA events
+    around plain calls, not graph replays."""
+    from hackathon_b200 import workload as W
+    out = {}
+    cases = [("2d_n1023_o6_k50_b64", 2, 1023, 6, [50.0], 64), ("2d_n2047_o6_b16", 2, 2047, 6, [10.0, 100.0, 400.0], 16),
+             ("3d_n255_o6_k30_b4", 3, 255, 6, [30.0], 4)]
+    for name, dim, n, order, ks, batch in cases:
+        if dim == 3:
+            f_host = np.stack([W.source_3d(n, W.sine_modes(4000 + b, 16, 64, dim=3))[1:-1, 1:-1, 1:-1]
+                               for b in range(batch)])
+        else:
+            f_host = np.stack([W.source_2d(n, W.sine_modes(5000 + b, 8, 20), fast=True)[1:-1, 1:-1]
+                               for b in range(batch)])
+        rhs = torch.from_numpy(np.ascontiguousarray(f_host)).cuda()
+        u, plain = torch.empty_like(rhs), torch.empty_like(rhs)
+        rec = {"iterations": [], "rel_residual": [], "max_rel_diff_vs_fp64": []}
+        t_plain = t_ref = 0.0
+        for k in ks:
+            p = hh.Plan.helmholtz(ctx, dim, n, order, k)
+            p.tune(batch)
+            p.solve(rhs, plain, batch)
+            p.solve_refined(rhs, u, batch)
+            torch.cuda.synchronize()
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            reps = 3
+            e0.record(st)
+            for _ in range(reps):
+                p.solve(rhs, plain, batch)
+            e1.record(st)
+            for _ in range(reps):
+                it, rr = p.solve_refined(rhs, u, batch)
+            e2.record(st)
+            e2.synchronize()
+            t_plain += e0.elapsed_time(e1) / reps
+            t_ref += e1.elapsed_time(e2) / reps
+            rec["iterations"].append(it)
+            rec["rel_residual"].append(rr)
+            d = (u - plain).abs().max() / plain.abs().max()
+            rec["max_rel_diff_vs_fp64"].append(float(d))
+            p.close()
+        solves = batch * len(ks)
+        rec["fp64_solves_per_s"] = solves / (t_plain / 1000.0)
+        rec["refined_solves_per_s"] = solves / (t_ref / 1000.0)
+        rec["refined_vs_fp64"] = rec["refined_solves_per_s"] / rec["fp64_solves_per_s"]
+        out[name] = rec
+        del rhs, u, plain
+        torch.cuda.empty_cache()
+    return out
+
+
 SERVE_2D = [63, 127, 255, 511, 1023, 2047]
 SERVE_3D = [31, 63, 127, 255]
 
@@ -457,6 +512,7 @@ def main():
         }
         if world == 1 and not args.no_secondary:
             line["secondary"] = secondary_configs(hh, ctx, st, torch)
+            line["secondary"]["mixed_precision_refined"] = refined_configs(hh, ctx, st, torch)
             line["secondary"]["serving"] = serve_run(hh, torch, seconds=1.0)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
