@@ -32,14 +32,19 @@ def _solo(ctx, dim, n, order, k, f):
 
 
 def test_mixed_stream_matches_solo_host_buffers(ctx):
-    reqs = _requests(1, 40)
-    srv = hh.Server(0, hbm_budget=8 << 30, streams=3)
-    bufs, ids = [], []
+    # the mixed stream, then a burst of requests of one plan (queued behind each other, so the
+    # loop has same-plan requests waiting to merge); buffers are pinned before submission so that
+    # submitting is fast next to solving
+    rng = np.random.default_rng(11)
+    burst = [(2, 63, 4, 5.0, 2, rng.standard_normal((2, 63, 63)) + 1j * rng.standard_normal((2, 63, 63)))
+             for _ in range(8)]
+    reqs = _requests(1, 40) + burst
+    bufs = []
     for dim, n, order, k, nrhs, f in reqs:
         fp = torch.from_numpy(f).pin_memory()
-        up = torch.empty_like(fp).pin_memory()
-        bufs.append((fp, up))
-        ids.append(srv.submit(dim, n, order, k, nrhs, fp, up))
+        bufs.append((fp, torch.empty_like(fp).pin_memory()))
+    srv = hh.Server(0, hbm_budget=8 << 30, streams=3)
+    ids = [srv.submit(dim, n, order, k, nrhs, fp, up) for (dim, n, order, k, nrhs, f), (fp, up) in zip(reqs, bufs)]
     infos = [srv.wait(i) for i in ids]
     stats = srv.stats()
     srv.close()
