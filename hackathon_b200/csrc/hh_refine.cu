@@ -33,35 +33,37 @@ __global__ void __launch_bounds__(256)
     const double2 *ub = u + b * field;
     const double2  zero = make_double2(0.0, 0.0);
     const long     plane = (long)n0 * n1;
-    double         mr = 0.0, mf = 0.0;
+    double         mr = 0.0, mf = 0.0; // squared moduli; the root is taken once per block
+    auto ld = [&](const double2 *q, bool ok) { return ok ? __ldg(q) : zero; };
     for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < field; p += (long)gridDim.x * blockDim.x) {
         const int  i = (int)(p % n0);
         const long rest = p / n0;
         const int  j = D3 ? (int)(rest % n1) : 0;
         const int  r = D3 ? (int)(rest / n1) : (int)rest;
-        auto U = [&](int di, int dj, int dr) -> double2 {
-            const int ii = i + di, jj = j + dj, rr = r + dr;
-            if (ii < 0 || ii >= n0 || jj < 0 || jj >= n1 || rr < 0 || rr >= n2) return zero;
-            return __ldg(ub + ii + (long)jj * n0 + (long)rr * plane);
-        };
-        double2 acc = zero;
+        const bool xl = i > 0, xr = i + 1 < n0, yl = D3 && j > 0, yr = D3 && j + 1 < n1;
+        double2    acc = zero;
 #pragma unroll
         for (int dr = -1; dr <= 1; dr++) {
+            if (r + dr < 0 || r + dr >= n2) continue; // the zero Dirichlet layer
             const double2 *T = dr < 0 ? subt : (dr == 0 ? diagt : supt);
-            acc = cadd(acc, cmul(__ldg(T + 3 * prow + r), U(0, 0, dr)));
-            acc = cadd(acc, cmul(__ldg(T + prow + r), cadd(U(-1, 0, dr), U(1, 0, dr))));
+            const double2 *c = ub + p + dr * plane;    // the neighbour (i, j, r + dr)
+            const double2  xs = cadd(ld(c - 1, xl), ld(c + 1, xr));
+            acc = cadd(acc, cmul(__ldg(T + 3 * prow + r), __ldg(c)));
+            acc = cadd(acc, cmul(__ldg(T + prow + r), xs));
             if constexpr (D3) {
-                const double2 corners = cadd(cadd(U(-1, -1, dr), U(1, -1, dr)), cadd(U(-1, 1, dr), U(1, 1, dr)));
+                const double2 ys = cadd(ld(c - n0, yl), ld(c + n0, yr));
+                const double2 corners = cadd(cadd(ld(c - n0 - 1, yl && xl), ld(c - n0 + 1, yl && xr)),
+                                             cadd(ld(c + n0 - 1, yr && xl), ld(c + n0 + 1, yr && xr)));
                 acc = cadd(acc, cmul(__ldg(T + r), corners));
-                acc = cadd(acc, cmul(__ldg(T + 2 * prow + r), cadd(U(0, -1, dr), U(0, 1, dr))));
+                acc = cadd(acc, cmul(__ldg(T + 2 * prow + r), ys));
             }
         }
         const double2 f = __ldg(rhs + b * field + p);
         const double2 rv = csub(acc, f);
         res[b * field + p] = rv;
         if (norms) {
-            mr = fmax(mr, hypot(rv.x, rv.y));
-            mf = fmax(mf, hypot(f.x, f.y));
+            mr = fmax(mr, fma(rv.x, rv.x, rv.y * rv.y));
+            mf = fmax(mf, fma(f.x, f.x, f.y * f.y));
         }
     }
     if (norms) {
@@ -77,8 +79,8 @@ __global__ void __launch_bounds__(256)
         __syncthreads();
         if (threadIdx.x == 0) {
             for (int x = 1; x < (int)(blockDim.x >> 5); x++) { mr = fmax(mr, sr[x]); mf = fmax(mf, sf[x]); }
-            atomic_max_nonneg(norms, mr);
-            atomic_max_nonneg(norms + 1, mf);
+            atomic_max_nonneg(norms, sqrt(mr));
+            atomic_max_nonneg(norms + 1, sqrt(mf));
         }
     }
 }
