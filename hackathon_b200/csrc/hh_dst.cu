@@ -429,12 +429,13 @@ __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 template <int M> struct WCfg;
 // TL lanes per line, R values per lane, WPC warps per CTA, NBUF line buffers per warp in the rows
 // kernel (2: the next line loads while one is transformed; 1: more warps per SM instead), MINB
-// CTAs per SM the register budget is sized for
-template <> struct WCfg<1024> { static constexpr int TL = 32, R = 32, WPC = 2, NBUF = 2, MINB = 3; };
-template <> struct WCfg<512>  { static constexpr int TL = 16, R = 32, WPC = 2, NBUF = 2, MINB = 3; };
-template <> struct WCfg<256>  { static constexpr int TL = 16, R = 16, WPC = 4, NBUF = 2, MINB = 3; };
-template <> struct WCfg<128>  { static constexpr int TL = 8,  R = 16, WPC = 4, NBUF = 2, MINB = 3; };
-template <> struct WCfg<64>   { static constexpr int TL = 8,  R = 8,  WPC = 4, NBUF = 2, MINB = 3; };
+// CTAs per SM the register budget is sized for; CWPC warps per CTA and CNT tiles per warp in the
+// columns kernel (CNT - 1 tiles load while one is transformed)
+template <> struct WCfg<1024> { static constexpr int TL = 32, R = 32, WPC = 2, NBUF = 2, MINB = 3, CWPC = 2, CNT = 2; };
+template <> struct WCfg<512>  { static constexpr int TL = 16, R = 32, WPC = 2, NBUF = 2, MINB = 3, CWPC = 2, CNT = 2; };
+template <> struct WCfg<256>  { static constexpr int TL = 16, R = 16, WPC = 4, NBUF = 2, MINB = 3, CWPC = 4, CNT = 2; };
+template <> struct WCfg<128>  { static constexpr int TL = 8,  R = 16, WPC = 4, NBUF = 2, MINB = 3, CWPC = 4, CNT = 2; };
+template <> struct WCfg<64>   { static constexpr int TL = 8,  R = 8,  WPC = 4, NBUF = 2, MINB = 3, CWPC = 4, CNT = 2; };
 
 template <int M> struct WGeom {
     static constexpr int TL = WCfg<M>::TL, R = WCfg<M>::R, WPC = WCfg<M>::WPC;
@@ -822,37 +823,38 @@ template <int M> struct WColGeom {
     static constexpr int TILE = (LPW * BR * NBOX + 7) / 8 * 8;
     // line exchange areas offset so that the LPW lines of an 8-lane phase fall on distinct banks
     static constexpr int BUFC = (G::BUF + 7) / 8 * 8 + (LPW > 1 ? 8 / LPW : 0);
-    static constexpr int WPC = G::WPC;
-    static constexpr int WARP_ELEMS = (2 * TILE + LPW * BUFC + 7) / 8 * 8; // two tiles, one exchange area
-    static constexpr int SMEM = 256 + 16 * WARP_ELEMS * WPC;               // + barriers, + base alignment
+    static constexpr int WPC = WCfg<M>::CWPC, NT = WCfg<M>::CNT;
+    static constexpr int WARP_ELEMS = (NT * TILE + LPW * BUFC + 7) / 8 * 8; // NT tiles, one exchange area
+    static constexpr int SMEM = 256 + 16 * WARP_ELEMS * WPC;                // + barriers, + base alignment
     static_assert(NBOX == 1 || (LPW * BR) % 8 == 0, "box offsets must stay 128-byte aligned");
+    static_assert(NT * WPC * 8 <= 128, "the barriers fit in front of the tiles");
 };
 
 template <int M, bool LP = false>
-__global__ void __launch_bounds__(32 * WCfg<M>::WPC, 3)
+__global__ void __launch_bounds__(32 * WCfg<M>::CWPC, 3)
     k_dst1_wc(const __grid_constant__ CUtensorMap in_map, const __grid_constant__ CUtensorMap out_map, long ncols,
               long nplanes, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
     using G = WGeom<M>;
     using CG = WColGeom<M>;
     constexpr int      TL = G::TL, LPW = G::LPW, KB = G::KB, N = M - 1, K2 = 2 * KB;
-    constexpr int      BR = CG::BR, NBOX = CG::NBOX;
+    constexpr int      BR = CG::BR, NBOX = CG::NBOX, NT = CG::NT;
     constexpr uint32_t kBoxBytes = LPW * BR * 16;
     extern __shared__ __align__(128) unsigned char dsm_raw[];
     // 128-byte aligned start of the tiles (the allocation carries 128 bytes of slack for this)
     unsigned char *dsm = dsm_raw + ((128u - (smem_u32(dsm_raw) & 127u)) & 127u);
     const int      lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
     const int      c = lane % LPW, l = lane / LPW; // interleaved: lane = c + LPW l
-    uint64_t      *bar = reinterpret_cast<uint64_t *>(dsm) + 2 * wq;
+    uint64_t      *bar = reinterpret_cast<uint64_t *>(dsm) + NT * wq;
     double2       *wbase = reinterpret_cast<double2 *>(dsm + 128) + wq * CG::WARP_ELEMS;
     if ((smem_u32(wbase) & 127u) != 0) { // cannot happen with the layout above; never issue a misaligned copy
         if (lane == 0) atomicExch(err, 2);
         return;
     }
-    double2   *xbuf = wbase + 2 * CG::TILE + c * CG::BUFC; // the line's exchange area
+    double2   *xbuf = wbase + NT * CG::TILE + c * CG::BUFC; // the line's exchange area
     const long cgroups = (ncols + LPW - 1) / LPW;
     const long groups = cgroups * nplanes;
-    const long stride = (long)gridDim.x * G::WPC;
-    const long g0 = (long)blockIdx.x * G::WPC + wq;
+    const long stride = (long)gridDim.x * CG::WPC;
+    const long g0 = (long)blockIdx.x * CG::WPC + wq;
     if (g0 >= groups) return; // whole warp
 
     auto fetch = [&](long grp, int s) {
@@ -862,25 +864,22 @@ __global__ void __launch_bounds__(32 * WCfg<M>::WPC, 3)
             tma_tile_load(wbase + s * CG::TILE + b * LPW * BR, &in_map, x0, b * BR, p, &bar[s]);
     };
     if (lane == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int u = 0; u < NT; u++) mbar_init(&bar[u], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncwarp();
-    if (lane == 0) {
-        fetch(g0, 0);
-        if (g0 + stride < groups) fetch(g0 + stride, 1);
-    }
+    if (lane == 0)
+        for (int u = 0; u < NT && g0 + u * stride < groups; u++) fetch(g0 + u * stride, u);
     WConst<M> K;
     K.load(l, tw, sn);
 
     int  it = 0;
     long failed = -1;
     for (long grp = g0; grp < groups; grp += stride, it++) {
-        const int s = it & 1;
+        const int s = it % NT;
         double2  *tile = wbase + s * CG::TILE;
         const bool live = (grp % cgroups) * LPW + c < ncols;
-        if (!mbar_wait_parity(&bar[s], (it >> 1) & 1)) {
+        if (!mbar_wait_parity(&bar[s], (it / NT) & 1)) {
             if (lane == 0) atomicExch(err, 1);
             failed = grp;
             break;
@@ -900,19 +899,18 @@ __global__ void __launch_bounds__(32 * WCfg<M>::WPC, 3)
             for (int b = 0; b < NBOX; b++) tma_tile_store(&out_map, x0, b * BR, pl, tile + b * LPW * BR);
             asm volatile("cp.async.bulk.commit_group;" ::: "memory");
             // the tile is read by the store before the next load overwrites it
-            if (grp + 2 * stride < groups) {
+            if (grp + NT * stride < groups) {
                 asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-                fetch(grp + 2 * stride, s);
+                fetch(grp + NT * stride, s);
             }
         }
         __syncwarp();
     }
     if (lane == 0) {
         asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); // stores complete before exit
-        if (failed >= 0) {
-            mbar_wait_parity(&bar[it & 1], (it >> 1) & 1);
-            if (failed + stride < groups) mbar_wait_parity(&bar[(it + 1) & 1], ((it + 1) >> 1) & 1);
-        }
+        if (failed >= 0) // copies still in flight get a bounded chance to land
+            for (int j = 0; j < NT && failed + j * stride < groups; j++)
+                mbar_wait_parity(&bar[(it + j) % NT], ((it + j) / NT) & 1);
     }
 }
 
@@ -1169,10 +1167,10 @@ static int launch_wc(Ctx *c, long ncols, long planes, const double2 *in, long ld
     int dev = 0, sms = 148, per_sm = 0;
     HH_CUDA(cudaGetDevice(&dev));
     HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * G::WPC, CG::SMEM));
+    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * CG::WPC, CG::SMEM));
     const long groups = (ncols + G::LPW - 1) / G::LPW * planes;
-    const long ctas = std::min<long>((groups + G::WPC - 1) / G::WPC, (long)std::max(1, per_sm) * sms);
-    kern<<<(unsigned)ctas, 32 * G::WPC, CG::SMEM, c->stream>>>(in_map, out_map, ncols, planes, tw, sn, c->err_word);
+    const long ctas = std::min<long>((groups + CG::WPC - 1) / CG::WPC, (long)std::max(1, per_sm) * sms);
+    kern<<<(unsigned)ctas, 32 * CG::WPC, CG::SMEM, c->stream>>>(in_map, out_map, ncols, planes, tw, sn, c->err_word);
     HH_CUDA(cudaGetLastError());
     c->launches++;
     return HH_OK;
