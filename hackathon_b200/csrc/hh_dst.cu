@@ -430,12 +430,13 @@ template <int M> struct WCfg;
 // TL lanes per line, R values per lane, WPC warps per CTA, NBUF line buffers per warp in the rows
 // kernel (2: the next line loads while one is transformed; 1: more warps per SM instead), MINB
 // CTAs per SM the register budget is sized for; CWPC warps per CTA and CNT tiles per warp in the
-// columns kernel (CNT - 1 tiles load while one is transformed)
-template <> struct WCfg<1024> { static constexpr int TL = 32, R = 32, WPC = 2, NBUF = 2, MINB = 3, CWPC = 2, CNT = 2; };
-template <> struct WCfg<512>  { static constexpr int TL = 16, R = 32, WPC = 2, NBUF = 2, MINB = 3, CWPC = 2, CNT = 2; };
-template <> struct WCfg<256>  { static constexpr int TL = 16, R = 16, WPC = 4, NBUF = 2, MINB = 3, CWPC = 4, CNT = 2; };
-template <> struct WCfg<128>  { static constexpr int TL = 8,  R = 16, WPC = 4, NBUF = 2, MINB = 3, CWPC = 4, CNT = 2; };
-template <> struct WCfg<64>   { static constexpr int TL = 8,  R = 8,  WPC = 4, NBUF = 2, MINB = 3, CWPC = 4, CNT = 2; };
+// columns kernel (CNT - 1 tiles load while one is transformed); RING: the rows use the CTA-ring
+// kernel with RWPC warps per CTA
+template <> struct WCfg<1024> { static constexpr int TL = 32, R = 32, WPC = 2, NBUF = 2, MINB = 3, CWPC = 2, CNT = 2, RWPC = 4, RING = 1; };
+template <> struct WCfg<512>  { static constexpr int TL = 16, R = 32, WPC = 2, NBUF = 2, MINB = 3, CWPC = 2, CNT = 2, RWPC = 4, RING = 0; };
+template <> struct WCfg<256>  { static constexpr int TL = 16, R = 16, WPC = 4, NBUF = 2, MINB = 3, CWPC = 4, CNT = 2, RWPC = 4, RING = 0; };
+template <> struct WCfg<128>  { static constexpr int TL = 8,  R = 16, WPC = 4, NBUF = 2, MINB = 3, CWPC = 4, CNT = 2, RWPC = 4, RING = 0; };
+template <> struct WCfg<64>   { static constexpr int TL = 8,  R = 8,  WPC = 4, NBUF = 2, MINB = 3, CWPC = 4, CNT = 2, RWPC = 4, RING = 0; };
 
 template <int M> struct WGeom {
     static constexpr int TL = WCfg<M>::TL, R = WCfg<M>::R, WPC = WCfg<M>::WPC;
@@ -808,6 +809,113 @@ __global__ void __launch_bounds__(32 * WCfg<M>::WPC, WCfg<M>::MINB)
     }
 }
 
+// ---- rows, CTA ring: the same transform with the line buffers pooled per CTA.  RWPC warps share
+// RNS = RWPC + 2 buffers: ticket t of the CTA (group blockIdx.x + t gridDim.x) lives in buffer
+// t % RNS; warp w takes tickets w, w + RWPC, ...; the warp that finishes ticket t brings in
+// ticket t + RNS to the buffer it frees.  With fewer buffers per warp than the per-warp double
+// buffer (1.5 against 2), more warps fit per SM.  gen[b] counts the copies issued to buffer b, so
+// a warp waits on a buffer's mbarrier only once the copy of its ticket has been issued (at most
+// one phase ahead of the barrier).
+template <int M> struct WRing {
+    using G = WGeom<M>;
+    static constexpr int WPC = WCfg<M>::RWPC, NS = WPC + 2;
+    static constexpr int SLOT = G::LPW * G::BUF;        // elements of one buffer (one line group)
+    static constexpr int SMEM = 128 + 16 * NS * SLOT;   // barriers and counters, then the buffers
+    static_assert(NS * 8 + NS * 4 <= 128, "barriers and counters fit in front of the buffers");
+};
+
+template <int M, bool LP = false>
+__global__ void __launch_bounds__(32 * WCfg<M>::RWPC, 2)
+    k_dst1_wr(const double2 *in, double2 *out, long nlines, long nplanes, long in_ld, long out_ld, long in_plane,
+              long out_plane, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
+    using G = WGeom<M>;
+    using RG = WRing<M>;
+    constexpr int      TL = G::TL, LPW = G::LPW, KB = G::KB, BUF = G::BUF, N = M - 1, K2 = 2 * KB;
+    constexpr int      NS = RG::NS, WPC = RG::WPC;
+    constexpr uint32_t kLineBytes = N * 16;
+    extern __shared__ __align__(128) unsigned char dsm[];
+    const int          lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+    const int          c = lane / TL, l = lane % TL;
+    uint64_t          *bar = reinterpret_cast<uint64_t *>(dsm);
+    volatile int      *gen = reinterpret_cast<volatile int *>(dsm + 8 * NS);
+    double2           *slots = reinterpret_cast<double2 *>(dsm + 128);
+    const long         total = nlines * nplanes;
+    const long         groups = (total + LPW - 1) / LPW;
+    if ((long)blockIdx.x >= groups) return; // whole CTA
+    const long tickets = (groups - blockIdx.x + gridDim.x - 1) / gridDim.x;
+    auto       grp_of = [&](long t) { return (long)blockIdx.x + t * gridDim.x; };
+    auto       src_of = [&](long g) { return in + (g / nlines) * in_plane + (g % nlines) * in_ld; };
+    auto       dst_of = [&](long g) { return out + (g / nlines) * out_plane + (g % nlines) * out_ld; };
+    auto       fetch = [&](long t) { // lane 0: ticket t into buffer t % NS
+        const int  b = (int)(t % NS);
+        const long first = grp_of(t) * LPW;
+        const int  nl = (int)((total - first) < LPW ? (total - first) : LPW);
+        mbar_expect_tx(&bar[b], (uint32_t)nl * kLineBytes);
+        for (int x = 0; x < nl; x++)
+            tma_bulk_load(slots + (long)b * RG::SLOT + x * BUF, src_of(first + x), kLineBytes, &bar[b]);
+    };
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < NS; b++) {
+            mbar_init(&bar[b], 1);
+            gen[b] = 0;
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (int b = 0; b < NS && b < tickets; b++) {
+            fetch(b);
+            gen[b] = 1;
+        }
+    }
+    __syncthreads();
+    WConst<M> K;
+    K.load(l, tw, sn);
+
+    long failed = -1;
+    for (long t = wq; t < tickets; t += WPC) {
+        const int b = (int)(t % NS);
+        const int want = (int)(t / NS) + 1; // the copy of this ticket is buffer b's want-th
+        bool      ok = true;
+        if (lane == 0) {
+            long spin = 0;
+            while (gen[b] < want && ++spin < (1L << 26)) {
+            }
+            ok = gen[b] >= want;
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0) && mbar_wait_parity(&bar[b], (uint32_t)((t / NS) & 1));
+        if (!ok) {
+            if (lane == 0) atomicExch(err, 1);
+            failed = t;
+            break;
+        }
+        double2   *buf = slots + (long)b * RG::SLOT + c * BUF;
+        const long line = grp_of(t) * LPW + c;
+        const bool live = line < total;
+        if constexpr (LP) w_transform_lp<M, false>([&](int j) { return buf[j - 1]; }, buf, l, live, K);
+        else w_transform<M, false>([&](int j) { return buf[j - 1]; }, buf, l, live, K);
+        if (live) {
+            double2 *dst = dst_of(line);
+#pragma unroll
+            for (int q = 0; q < M / TL; q++) {
+                const int p = l + TL * q;
+                if (p < N) dst[p] = buf[(K2 + 1) * (p / K2) + p % K2];
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // reads before the refill
+        __syncwarp();
+        if (lane == 0 && t + NS < tickets) {
+            fetch(t + NS);
+            __threadfence_block(); // the copy's arrival is registered before its ticket is announced
+            gen[b] = want + 1;
+        }
+    }
+    // after an expired wait, copies this warp issued get a bounded chance to land before the
+    // CTA's shared memory is released
+    if (failed >= 0 && lane == 0)
+        for (long t = failed; t < tickets && t < failed + NS; t++) {
+            const int b = (int)(t % NS);
+            if (gen[b] >= (int)(t / NS) + 1) mbar_wait_parity(&bar[b], (uint32_t)((t / NS) & 1));
+        }
+}
+
 // ---- columns: line x of plane p is element j at base + p plane + x + (j - 1) ld.  A 4-D tensor
 // map (re/im, x, j, plane) brings C = LPW neighbouring columns, all rows, into a [j][c] tile; the
 // warp's lanes interleave over the C lines (lane = c + LPW l) so that reading the tile is free of
@@ -1034,7 +1142,27 @@ template <int M, bool IS, bool OS> static int launch_fft(Ctx *c, const DstArgs &
     return HH_OK;
 }
 
-template <int M, bool LP> static int launch_w(Ctx *c, const DstArgs &a) {
+template <int M, bool LP> static int launch_wr(Ctx *c, const DstArgs &a) {
+    using G = WGeom<M>;
+    using RG = WRing<M>;
+    const double2 *tw;
+    const double  *sn;
+    HH_TRY(tables_for(c, M, &tw, &sn));
+    HH_CUDA(cudaFuncSetAttribute(k_dst1_wr<M, LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, RG::SMEM));
+    int dev = 0, sms = 148, per_sm = 0;
+    HH_CUDA(cudaGetDevice(&dev));
+    HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dst1_wr<M, LP>, 32 * RG::WPC, RG::SMEM));
+    const long groups = (a.nlines * a.planes + G::LPW - 1) / G::LPW;
+    const long ctas = std::min<long>((groups + RG::WPC - 1) / RG::WPC, (long)std::max(1, per_sm) * sms);
+    k_dst1_wr<M, LP><<<(unsigned)ctas, 32 * RG::WPC, RG::SMEM, c->stream>>>(
+        a.in, a.out, a.nlines, a.planes, a.in_ld, a.out_ld, a.in_plane, a.out_plane, tw, sn, c->err_word);
+    HH_CUDA(cudaGetLastError());
+    c->launches++;
+    return HH_OK;
+}
+
+template <int M, bool LP> static int launch_wp(Ctx *c, const DstArgs &a) {
     using G = WGeom<M>;
     const double2 *tw;
     const double  *sn;
@@ -1051,6 +1179,11 @@ template <int M, bool LP> static int launch_w(Ctx *c, const DstArgs &a) {
     HH_CUDA(cudaGetLastError());
     c->launches++;
     return HH_OK;
+}
+
+template <int M, bool LP> static int launch_w(Ctx *c, const DstArgs &a) {
+    if constexpr (WCfg<M>::RING) return launch_wr<M, LP>(c, a);
+    else return launch_wp<M, LP>(c, a);
 }
 
 // LP: single-precision arithmetic where the persistent-warp kernels serve (n + 1 = 64 .. 1024);
