@@ -32,6 +32,20 @@ def test_dst_rows_matches_oracle(ctx, oracle, n):
     assert rel_err(_host(dst), oracle.dst1_rows(x)) < 1e-13
 
 
+@pytest.mark.parametrize("rows", [1, 5, 6, 7, 2999, 5001])
+def test_dst_rows_1023_ring_ticket_counts(ctx, oracle, rows):
+    """1023-point rows go through the CTA-ring kernel (four warps sharing six line buffers):
+    fewer tickets per block than buffers, exactly as many, one more, and thousands of rows whose
+    tickets fall unevenly on the blocks."""
+    n = 1023
+    rng = np.random.default_rng(rows)
+    x = rng.standard_normal((rows, n)) + 1j * rng.standard_normal((rows, n))
+    src, dst = _dev(x), torch.empty((rows, n), dtype=torch.complex128, device="cuda")
+    ctx.dst1_rows(n, rows, src, dst)
+    ctx.synchronize()
+    assert rel_err(_host(dst), oracle.dst1_rows(x)) < 1e-13
+
+
 def test_dst_rows_golden_and_in_place(ctx):
     g = golden("dst_rows.npz")
     for n in (1, 7, 31, 63, 100):
