@@ -32,11 +32,12 @@ def test_dst_rows_matches_oracle(ctx, oracle, n):
     assert rel_err(_host(dst), oracle.dst1_rows(x)) < 1e-13
 
 
-@pytest.mark.parametrize("rows", [1, 5, 6, 7, 2999, 5001])
+@pytest.mark.parametrize("rows", [1, 5, 1776, 1777, 2072, 5001])
 def test_dst_rows_1023_ring_ticket_counts(ctx, oracle, rows):
-    """1023-point rows go through the CTA-ring kernel (four warps sharing six line buffers):
-    fewer tickets per block than buffers, exactly as many, one more, and thousands of rows whose
-    tickets fall unevenly on the blocks."""
+    """1023-point rows go through the CTA-ring kernel (four warps sharing six line buffers, at
+    most two blocks per SM, so 296 blocks on 148 SMs): fewer tickets per block than buffers,
+    exactly as many (1776 rows), one block with one more, one more each, and thousands of rows
+    whose tickets fall unevenly on the blocks."""
     n = 1023
     rng = np.random.default_rng(rows)
     x = rng.standard_normal((rows, n)) + 1j * rng.standard_normal((rows, n))
