@@ -52,6 +52,14 @@ def sources(count: int, index: int = 1) -> np.ndarray:
     return out
 
 
+def aggregate_over_ranks(ms_local: float, batch: int, steps: int, world: int, reduce_max) -> tuple:
+    """Whole-job throughput of `world` replicas (each rank solves its own batch, no data-path
+    collective): the slowest rank's device time bounds the job.  reduce_max(x) returns the max
+    of x over the ranks (an all_reduce); returns (ms_max, solves/s over all ranks)."""
+    ms_max = reduce_max(ms_local) if world > 1 else ms_local
+    return ms_max, world * batch * steps / (ms_max / 1000.0)
+
+
 class ClockSampler:
     """nvidia-smi samples (SM clock, throttle reasons) during the timed region."""
 
@@ -440,11 +448,13 @@ def main():
     clk = sampler
     launches = kernels_per_step * args.steps
     ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
+
+    def reduce_max(x: float) -> float:
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * batch * args.steps / (ms_max / 1000.0)
+        return float(t.item())
+
+    ms_max, value = aggregate_over_ranks(ms, batch, args.steps, world, reduce_max)
 
     # per-kernel device time: a second pass with CUDA events around each stage on the same stream
     ctx.stage_times()
