@@ -760,21 +760,23 @@ static int solve_host_common(hh_plan *pl, const double *in_host, double *out_hos
         HH_CUDA(cudaMalloc(&owner->stage, sizeof(double2) * (size_t)need));
         owner->stage_elems = need;
     }
-    // chunks of at least 4 MB of field data, at most 8 chunks
-    int nchunk = (int)std::min<long>(8, std::max<long>(1, (long)(sizeof(double2) * need) / (4L << 20)));
+    // chunks of at least 4 MB of field data, at most kMaxChunks: more chunks shorten the
+    // pipeline's fill (first copy in) and drain (last copy out)
+    constexpr int kMaxChunks = 16;
+    int nchunk = (int)std::min<long>(kMaxChunks, std::max<long>(1, (long)(sizeof(double2) * need) / (4L << 20)));
     nchunk = std::min(nchunk, batch);
     if (!c->copy_in) {
         HH_CUDA(cudaStreamCreateWithFlags(&c->copy_in, cudaStreamNonBlocking));
         HH_CUDA(cudaStreamCreateWithFlags(&c->copy_out, cudaStreamNonBlocking));
     }
-    while ((int)c->chunk_ev.size() < 2 * 8 + 1) {
+    while ((int)c->chunk_ev.size() < 2 * kMaxChunks + 1) {
         cudaEvent_t e;
         HH_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         c->chunk_ev.push_back(e);
     }
     // copies start after the work already queued on the context stream
-    HH_CUDA(cudaEventRecord(c->chunk_ev[16], c->stream));
-    HH_CUDA(cudaStreamWaitEvent(c->copy_in, c->chunk_ev[16], 0));
+    HH_CUDA(cudaEventRecord(c->chunk_ev[2 * kMaxChunks], c->stream));
+    HH_CUDA(cudaStreamWaitEvent(c->copy_in, c->chunk_ev[2 * kMaxChunks], 0));
     const int per = (batch + nchunk - 1) / nchunk;
     for (int i = 0, b0 = 0; b0 < batch; i++, b0 += per) {
         const int    nb = std::min(per, batch - b0);
@@ -790,8 +792,8 @@ static int solve_host_common(hh_plan *pl, const double *in_host, double *out_hos
         HH_CUDA(cudaMemcpyAsync(out_host + 2 * off, d, bytes, cudaMemcpyDeviceToHost, c->copy_out));
     }
     // the context stream sees the copies complete before anything queued after this call
-    HH_CUDA(cudaEventRecord(c->chunk_ev[16], c->copy_out));
-    HH_CUDA(cudaStreamWaitEvent(c->stream, c->chunk_ev[16], 0));
+    HH_CUDA(cudaEventRecord(c->chunk_ev[2 * kMaxChunks], c->copy_out));
+    HH_CUDA(cudaStreamWaitEvent(c->stream, c->chunk_ev[2 * kMaxChunks], 0));
     return hh_ctx_synchronize(owner);
 }
 
