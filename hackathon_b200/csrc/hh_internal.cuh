@@ -110,7 +110,7 @@ struct Plan {
     // reciprocal Thomas pivot of the row before each 16-row segment, [segment][line]
     double2 *Pv = nullptr;
     bool     const_rows = false; // stencil row tables constant along the line
-    int      variant = 0;        // line-solve kernel: 0/1 general (512x1, 256x2), 2..4 symmetric
+    int      variant = 0;        // line-solve kernel: 0/1 general (512x1, 256x2), 2..6 symmetric
     bool     sym = false;        // const_rows and sub == super on every line (constant k)
     bool     pf_ok = false;      // order-6 partial fractions well conditioned on every line
     double2 *subt = nullptr, *diagt = nullptr; // sub/diagonal row tables (4 * rows each)
