@@ -746,8 +746,13 @@ __global__ void __launch_bounds__(32 * WCfg<M>::WPC, WCfg<M>::MINB)
     const long g0 = (long)blockIdx.x * G::WPC + wq;
     if (g0 >= groups) return; // whole warp
 
-    auto src_of = [&](long g) { return in + (g / nlines) * in_plane + (g % nlines) * in_ld; };
-    auto dst_of = [&](long g) { return out + (g / nlines) * out_plane + (g % nlines) * out_ld; };
+    // one plane (all 2D calls): no 64-bit division per line
+    auto src_of = [&](long g) {
+        return nplanes == 1 ? in + g * in_ld : in + (g / nlines) * in_plane + (g % nlines) * in_ld;
+    };
+    auto dst_of = [&](long g) {
+        return nplanes == 1 ? out + g * out_ld : out + (g / nlines) * out_plane + (g % nlines) * out_ld;
+    };
     // lane 0: bring in line group `grp` to buffer set `s`
     auto fetch = [&](long grp, int s) {
         const long first = grp * LPW;
@@ -842,11 +847,15 @@ __global__ void __launch_bounds__(32 * WCfg<M>::RWPC, 2)
     const long         total = nlines * nplanes;
     const long         groups = (total + LPW - 1) / LPW;
     if ((long)blockIdx.x >= groups) return; // whole CTA
-    const long tickets = (groups - blockIdx.x + gridDim.x - 1) / gridDim.x;
-    auto       grp_of = [&](long t) { return (long)blockIdx.x + t * gridDim.x; };
-    auto       src_of = [&](long g) { return in + (g / nlines) * in_plane + (g % nlines) * in_ld; };
-    auto       dst_of = [&](long g) { return out + (g / nlines) * out_plane + (g % nlines) * out_ld; };
-    auto       fetch = [&](long t) { // lane 0: ticket t into buffer t % NS
+    const int  tickets = (int)((groups - blockIdx.x + gridDim.x - 1) / gridDim.x);
+    auto       grp_of = [&](int t) { return (long)blockIdx.x + (long)t * gridDim.x; };
+    auto       src_of = [&](long g) { // one plane (all 2D calls): no 64-bit division per line
+        return nplanes == 1 ? in + g * in_ld : in + (g / nlines) * in_plane + (g % nlines) * in_ld;
+    };
+    auto dst_of = [&](long g) {
+        return nplanes == 1 ? out + g * out_ld : out + (g / nlines) * out_plane + (g % nlines) * out_ld;
+    };
+    auto       fetch = [&](int t) { // lane 0: ticket t into buffer t % NS
         const int  b = (int)(t % NS);
         const long first = grp_of(t) * LPW;
         const int  nl = (int)((total - first) < LPW ? (total - first) : LPW);
@@ -869,10 +878,10 @@ __global__ void __launch_bounds__(32 * WCfg<M>::RWPC, 2)
     WConst<M> K;
     K.load(l, tw, sn);
 
-    long failed = -1;
-    for (long t = wq; t < tickets; t += WPC) {
-        const int b = (int)(t % NS);
-        const int want = (int)(t / NS) + 1; // the copy of this ticket is buffer b's want-th
+    int failed = -1;
+    for (int t = wq; t < tickets; t += WPC) {
+        const int b = t % NS;
+        const int want = t / NS + 1; // the copy of this ticket is buffer b's want-th
         bool      ok = true;
         if (lane == 0) {
             long spin = 0;
@@ -910,9 +919,9 @@ __global__ void __launch_bounds__(32 * WCfg<M>::RWPC, 2)
     // after an expired wait, copies this warp issued get a bounded chance to land before the
     // CTA's shared memory is released
     if (failed >= 0 && lane == 0)
-        for (long t = failed; t < tickets && t < failed + NS; t++) {
-            const int b = (int)(t % NS);
-            if (gen[b] >= (int)(t / NS) + 1) mbar_wait_parity(&bar[b], (uint32_t)((t / NS) & 1));
+        for (int t = failed; t < tickets && t < failed + NS; t++) {
+            const int b = t % NS;
+            if (gen[b] >= t / NS + 1) mbar_wait_parity(&bar[b], (uint32_t)((t / NS) & 1));
         }
 }
 
