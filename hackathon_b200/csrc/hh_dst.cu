@@ -973,9 +973,21 @@ __global__ void __launch_bounds__(32 * WCfg<M>::CWPC, 3)
     const long stride = (long)gridDim.x * CG::WPC;
     const long g0 = (long)blockIdx.x * CG::WPC + wq;
     if (g0 >= groups) return; // whole warp
+    // first column x0 and plane p of group g (32-bit division whenever the groups allow it)
+    auto coords = [&](long g, int &x0, int &p) {
+        if (groups < (1L << 31)) {
+            const unsigned gq = (unsigned)g, cg = (unsigned)cgroups;
+            x0 = (int)(gq % cg) * LPW;
+            p = (int)(gq / cg);
+        } else {
+            x0 = (int)((g % cgroups) * LPW);
+            p = (int)(g / cgroups);
+        }
+    };
 
     auto fetch = [&](long grp, int s) {
-        const int x0 = (int)((grp % cgroups) * LPW), p = (int)(grp / cgroups);
+        int x0, p;
+        coords(grp, x0, p);
         mbar_expect_tx(&bar[s], NBOX * kBoxBytes);
         for (int b = 0; b < NBOX; b++)
             tma_tile_load(wbase + s * CG::TILE + b * LPW * BR, &in_map, x0, b * BR, p, &bar[s]);
@@ -995,7 +1007,9 @@ __global__ void __launch_bounds__(32 * WCfg<M>::CWPC, 3)
     for (long grp = g0; grp < groups; grp += stride, it++) {
         const int s = it % NT;
         double2  *tile = wbase + s * CG::TILE;
-        const bool live = (grp % cgroups) * LPW + c < ncols;
+        int        gx0, gpl;
+        coords(grp, gx0, gpl);
+        const bool live = gx0 + c < ncols;
         if (!mbar_wait_parity(&bar[s], (it / NT) & 1)) {
             if (lane == 0) atomicExch(err, 1);
             failed = grp;
@@ -1012,8 +1026,7 @@ __global__ void __launch_bounds__(32 * WCfg<M>::CWPC, 3)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // tile writes before the store reads
         __syncwarp();
         if (lane == 0) {
-            const int x0 = (int)((grp % cgroups) * LPW), pl = (int)(grp / cgroups);
-            for (int b = 0; b < NBOX; b++) tma_tile_store(&out_map, x0, b * BR, pl, tile + b * LPW * BR);
+            for (int b = 0; b < NBOX; b++) tma_tile_store(&out_map, gx0, b * BR, gpl, tile + b * LPW * BR);
             asm volatile("cp.async.bulk.commit_group;" ::: "memory");
             // the tile is read by the store before the next load overwrites it
             if (grp + NT * stride < groups) {
