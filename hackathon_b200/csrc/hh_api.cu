@@ -348,7 +348,8 @@ static int plan_factor(hh_plan *pl, const std::vector<double2> &sub, const std::
     };
     p.const_rows = constant(sub) && constant(dia) && constant(sup);
     // symmetric constant lines (sub == super): the specialised solve; for order 6 it also needs
-    // |10 s - d| well away from zero on every line (partial fractions of A^-1 T^-1)
+    // |10 s - d| well away from zero on every line (partial fractions of A^-1 T^-1), and s not
+    // negligible beside d (the kernel re-forms 1/P as (1/s) (s / P))
     p.sym = p.const_rows;
     for (int k = 0; k < 4 && p.sym; k++) {
         const double2 a = sub[(size_t)k * p.rows], b = sup[(size_t)k * p.rows];
@@ -363,7 +364,8 @@ static int plan_factor(hh_plan *pl, const std::vector<double2> &sub, const std::
         };
         const double2 s = line_value(sub), d = line_value(dia);
         const double  num = std::hypot(10.0 * s.x - d.x, 10.0 * s.y - d.y);
-        p.pf_ok = num >= 0.25 * std::max(std::hypot(s.x, s.y), std::hypot(d.x, d.y));
+        const double  as = std::hypot(s.x, s.y), ad = std::hypot(d.x, d.y);
+        p.pf_ok = num >= 0.25 * std::max(as, ad) && as > 1e-6 * ad;
     }
     if (p.sym) p.variant = 2;
     // tables are [4][prow], zero past the last row (neutral rows in the solve)

@@ -645,8 +645,8 @@ __device__ __forceinline__ double lds_keep(const double *p) {
     return v;
 }
 
-// Order 6 with 16-row segments keeps the reciprocal pivots in shared memory, one column per
-// thread: in registers they would not fit beside the two solves' rows.
+// Order 6 with 16-row segments keeps its per-row multipliers tau_k = s ui_k in shared memory,
+// one column per thread: in registers they would not fit beside the two solves' rows.
 template <int SRC, int KS> struct SymUIS {
     static constexpr bool value = SRC == 6 && KS >= 16;
 };
@@ -721,25 +721,29 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
     static_assert(CW * NR <= 128 && NT >= 256, "cross-warp thread ranges");
     const int     t = threadIdx.x;
     const double2 zero = make_double2(0.0, 0.0);
-    // reciprocal pivot of row r0 + k: in registers, or (order 6 with 16-row segments, where the
-    // two solves' rows fill the registers) in shared memory, one column per thread
+    // Orders 0-4 keep the forward multipliers L_k and the reciprocal pivots ui_k in registers.
+    // Order 6, where the two solves' rows fill the registers, keeps one value per row instead:
+    // tau_k = s ui_k (= L_{k+1}), in the ui array or (16-row segments) in shared memory, one
+    // column per thread.  The sweeps read their multipliers from it as they are, and the final
+    // forward pass re-forms ui_k = (1/s) tau_k off the recurrence.
     constexpr bool UIS = SymUIS<SRC, KS>::value;
-    auto UI = [&](int k) -> double2 {
+    constexpr bool KEEP_L = SRC != 6;
+    auto TV = [&](int k) -> double2 {
         if constexpr (UIS) return lds_keep(uis + k * NT + t);
         else return ui[k];
     };
-    // forward multiplier of row r0 + k: kept in registers, or (order 6, where registers are
-    // short) re-formed from the reciprocal pivots as the set-up does
-    constexpr bool KEEP_L = SRC != 6;
+    const double2 tau_in = cmul(s, ui_in); // L_0 = s / P of row r0 - 1
+    const double2 rs = KEEP_L ? s : crcp(s);
+    // forward multiplier of row r0 + k
     auto LF = [&](int k) -> double2 {
         if constexpr (KEEP_L) return Lr[k];
-        else return cmul(s, k == 0 ? ui_in : UI(k - 1));
+        else return k == 0 ? tau_in : TV(k - 1);
     };
     // backward multiplier of row r0 + k, tau_k = s ui_k (= L_{k+1} where that row exists)
     const double2 tau_last = KEEP_L ? cmul(s, ui[KS - 1]) : s;
     auto TAU = [&](int k) -> double2 {
         if constexpr (KEEP_L) return k + 1 < KS ? Lr[k + 1] : tau_last;
-        else return cmul(s, UI(k));
+        else return TV(k);
     };
     // Pade factors of row r0 + k: the constants in warps whose rows all lie in [9, rows)
     auto PL = [&](int k) -> double {
@@ -897,12 +901,19 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
                 if constexpr (SRC == 6) z[r] = zaxpy(bfe[r], aeF, sm.eF[r][w][c]);
             }
             // the rows keep ui_k y_k, so that the back substitution is x_k = ui_k y_k - tau_k x_{k+1}
-            double2 up = ui_in;
+            double2 tp = tau_in;
 #pragma unroll
             for (int k = 0; k < KS; k++) {
-                const double2 u = UI(k);
-                const double2 l = KEEP_L ? Lr[k] : cmul(s, up);
-                up = u;
+                double2 u, l;
+                if constexpr (KEEP_L) {
+                    u = ui[k];
+                    l = Lr[k];
+                } else {
+                    const double2 tk = TV(k);
+                    u = cmul(rs, tk);
+                    l = tp;
+                    tp = tk;
+                }
 #pragma unroll
                 for (int r = 0; r < NR; r++) {
                     y[r] = zfms(v[r][k], l, y[r]);
@@ -1049,7 +1060,7 @@ __global__ void __launch_bounds__(NT, MINB)
     double2 *tabF = pre + io_elems;                     // [LOG + 1][NT]
     double2 *tabB = tabF + (LOG + 1) * NT;              // [LOG + 1][NT]
     constexpr bool UIS = SymUIS<SRC, KS>::value;
-    double2 *uis = tabB + (LOG + 1) * NT;               // [KS][NT] (UIS)
+    double2 *uis = tabB + (LOG + 1) * NT;               // [KS][NT] tau_k (UIS)
     double  *ttF = reinterpret_cast<double *>(uis + (UIS ? KS * NT : 0)); // [LOG + 1][NT] (order 6)
     double  *ttB = ttF + (LOG + 1) * NT;
     (void)HALO;
@@ -1104,10 +1115,13 @@ __global__ void __launch_bounds__(NT, MINB)
                 else ui[k] = factor_step(s, d, s, uprev, Lr[k]);
             }
             uprev = ui[k];
-            if constexpr (UIS) uis[k * NT + t] = ui[k];
             Af = cmul(Af, make_double2(-Lr[k].x, -Lr[k].y));
             const double2 tau = cmul(s, ui[k]);
             Ab = cmul(Ab, make_double2(-tau.x, -tau.y));
+            if constexpr (SRC == 6) { // order 6 keeps tau_k in place of ui_k
+                if constexpr (UIS) uis[k * NT + t] = tau;
+                else ui[k] = tau;
+            }
         }
     }
 
