@@ -1,7 +1,8 @@
 // TMA and mbarrier helpers shared by the transform and line-solve kernels (sm_100a).
 //
 // Every wait is bounded: mbar_wait_parity polls at most 2^26 times and reports failure, so a
-// copy that never lands cannot hang a kernel.  No helper uses cluster multicast.
+// copy that never lands cannot hang a kernel.  Every copy lands in the issuing CTA's own
+// shared memory only.
 #ifndef HH_TMA_CUH
 #define HH_TMA_CUH
 
