@@ -94,6 +94,25 @@ def test_every_line_solve_variant_matches_oracle(ctx, oracle, n, order, k):
     plan.close()
 
 
+@pytest.mark.parametrize("n,order,k", [(4095, 6, 100.0), (4095, 4, 400.0)])
+def test_solver2d_longest_lines_matches_oracle(ctx, oracle, n, order, k):
+    """The longest lines the symmetric kernel takes (4095 rows: 16-row segments, one line per
+    CTA, per-thread prefetch) beside the general kernel, and variant 2, whose 8-row segments
+    stop at 2048 rows and which therefore runs the general kernel here."""
+    f = _source(n, 11 * n + order)
+    ref = oracle.pipeline_2d(n, order, k, f)
+    plan = hh.Plan.helmholtz(ctx, 2, n, order, k)
+    outs = {}
+    for v in (0, 2, 5, 6):
+        plan.variant = v
+        outs[v] = plan.solve_source_host(f[1:-1, 1:-1])
+        assert_parity_2d(oracle, outs[v], ref, TOL)
+    assert np.array_equal(outs[2], outs[0])  # the same general kernel
+    assert np.array_equal(outs[6], outs[5])  # no tile input at one line per CTA
+    assert rel_err(outs[5], outs[0]) < TOL
+    plan.close()
+
+
 def test_symmetric_kernel_assembled_rhs(ctx, oracle):
     """Helmholtz plan on an assembled right-hand side (no fused operator) through the symmetric
     kernel, against the reference pipeline."""
