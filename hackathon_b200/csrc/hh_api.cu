@@ -367,7 +367,7 @@ static int plan_factor(hh_plan *pl, const std::vector<double2> &sub, const std::
         const double  as = std::hypot(s.x, s.y), ad = std::hypot(d.x, d.y);
         p.pf_ok = num >= 0.25 * std::max(as, ad) && as > 1e-6 * ad;
     }
-    if (p.sym) p.variant = 2;
+    if (p.sym) p.variant = sym_default_variant(p.rows);
     // tables are [4][prow], zero past the last row (neutral rows in the solve)
     auto padded = [&](const std::vector<double2> &t) {
         std::vector<double2> o(4 * (size_t)p.prow, make_double2(0.0, 0.0));

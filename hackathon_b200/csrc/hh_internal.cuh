@@ -140,6 +140,7 @@ int launch_residual(Plan *p, const double2 *u, const double2 *rhs, double2 *res,
 int launch_axpy(Ctx *c, double2 *u, const double2 *v, double s, long n); // u += s v
 int read_device_error(Ctx *c, int *val);
 int segment_count(int rows);
+int sym_default_variant(int rows);
 int padded_rows(int rows);
 int solve_variant_count();
 

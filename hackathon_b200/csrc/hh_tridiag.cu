@@ -1275,6 +1275,10 @@ static int launch_sym_src(Plan *p, const double2 *in, double2 *out, int batch) {
     }
 }
 
+// Default symmetric variant of a plan: 2, or 5 where the lines are longer than 8-row segments
+// reach (more than 256 * 8 rows), so that such plans keep the symmetric kernel untuned.
+int sym_default_variant(int rows) { return rows > 256 * kSeg ? 5 : 2; }
+
 bool sym_solve_supported(const Plan *p, int src_order) {
     const int max_rows = 256 * (p->variant >= 5 ? 16 : kSeg);
     return p->sym && p->rows <= max_rows && (src_order != 6 || (p->pf_ok && p->pade_l));

@@ -111,7 +111,8 @@ long hh_plan_field_size(const hh_plan *plan);  /* complex values per right-hand 
  * per SM), 3 (one block, no register cap), 4 (two right-hand sides per pass), 5 (16-row
  * segments) and 6 (16-row segments, right-hand sides brought in as TMA tiles).  hh_plan_tune
  * times each on `batch` right-hand sides and keeps the fastest (blocking; not during stream
- * capture); set/get select one directly. */
+ * capture); set/get select one directly.  A new symmetric plan starts at 2, or at 5 for lines
+ * longer than 2048 rows. */
 int hh_plan_tune(hh_plan *plan, int batch);
 int hh_plan_set_variant(hh_plan *plan, int variant);
 int hh_plan_variant(const hh_plan *plan);

@@ -102,6 +102,7 @@ def test_solver2d_longest_lines_matches_oracle(ctx, oracle, n, order, k):
     f = _source(n, 11 * n + order)
     ref = oracle.pipeline_2d(n, order, k, f)
     plan = hh.Plan.helmholtz(ctx, 2, n, order, k)
+    assert plan.variant == 5  # the default for lines beyond 2048 rows: the symmetric kernel
     outs = {}
     for v in (0, 2, 5, 6):
         plan.variant = v
@@ -144,9 +145,9 @@ def test_host_path_chunked_equals_device_path(ctx):
 @pytest.mark.parametrize("dim,n,order,batch", [(2, 1023, 4, 7), (2, 1023, 6, 5), (2, 511, 2, 9), (2, 127, 4, 3),
                                                (3, 63, 6, 3), (3, 127, 4, 2)])
 def test_tile_io_variant_equals_prefetch_variant(ctx, dim, n, order, batch):
-    """Variant 6 moves each right-hand side as TMA tiles (loads, and outside order 6 stores);
-    on device buffers of several right-hand sides, over every chunk boundary of the grid, its
-    result is bitwise variant 5's, whose arithmetic it shares."""
+    """Variant 6 brings each right-hand side in as TMA tiles.  On device buffers of several
+    right-hand sides, over every chunk boundary of the grid, its result is bitwise variant 5's,
+    whose arithmetic it shares."""
     torch = pytest.importorskip("torch")
     g = torch.Generator().manual_seed(1000 * dim + n + order)
     shape = (batch,) + (n,) * dim
