@@ -145,8 +145,8 @@ int hh_solve_source_host_noalloc(hh_plan *plan, const double *f_host, double *u_
 int hh_residual(hh_plan *plan, const double *sol_dev, const double *rhs_dev, double *res_dev, int batch,
                 double *max_res, double *max_rhs);
 
-/* Mixed-precision refined solve of `batch` assembled right-hand sides on the device (the
- * refined form of the survey's plan; the reference solves in plain FP64 only): every solve in
+/* Mixed-precision refined solve of `batch` assembled right-hand sides on the device (an
+ * addition: the reference solves in plain FP64 only): every solve in
  * the loop runs its DSTs in single-precision arithmetic (where n + 1 is a power of two up to
  * 1024; FP64 otherwise) and its line solves in FP64, and hh_residual's FP64 residual drives
  * the corrections:  u_0 = S(rhs),  u_{k+1} = u_k - S(A_h u_k - rhs)  until

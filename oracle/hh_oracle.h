@@ -3,7 +3,7 @@
  *
  * TEST INFRASTRUCTURE ONLY.  Nothing in the product (hackathon_b200/, include/) links,
  * loads or calls this code; only tests/, __graft_entry__.smoke() and bench.py's CPU
- * baseline leg use it, and only as the checker.
+ * baseline leg use it, and only to check results or to time the CPU baseline.
  *
  * Pinning: every function here is checked against the reference's own C sources built
  * unchanged into oracle/_ref/ (tests/golden/make_golden.py writes those outputs as
