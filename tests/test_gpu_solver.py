@@ -42,6 +42,31 @@ def test_solver2d_fused_source_matches_oracle(ctx, oracle, n, order, k):
     plan.close()
 
 
+@pytest.mark.parametrize("dim,n,order,k", [(2, 255, 6, 50 + 5j), (2, 1023, 4, 100 - 20j), (2, 127, 2, 30 + 30j),
+                                           (3, 31, 6, 20 + 3j), (3, 63, 4, 10 - 4j)])
+def test_complex_k_fused_source_matches_oracle(ctx, oracle, dim, n, order, k):
+    """Complex constant k (a damped or absorbing medium; the reference's problem structs carry
+    complex k): the fused operator and the shifted lines with complex k^2, for every line-solve
+    variant, against the reference pipeline."""
+    if dim == 2:
+        f = _source(n, 5 * n + order)
+        ref = oracle.pipeline_2d(n, order, k, f)
+        src = f[1:-1, 1:-1]
+    else:
+        f = W.source_3d(n, W.sine_modes(n + order, 16, min(n, 64), dim=3))
+        ref = oracle.pipeline_3d(n, order, k, f)
+        src = f[1:-1, 1:-1, 1:-1]
+    plan = hh.Plan.helmholtz(ctx, dim, n, order, k)
+    for v in range(7):
+        plan.variant = v
+        u = plan.solve_source_host(src)
+        if dim == 2:
+            assert_parity_2d(oracle, u, ref, TOL)
+        else:
+            assert rel_err(u, ref["sol"]) < TOL
+    plan.close()
+
+
 def test_readme_case_against_golden_and_exact(ctx):
     """./Direct_Solver 6 100 class: the reference's own output (golden) and the manufactured
     exact solution."""
