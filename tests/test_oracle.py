@@ -187,10 +187,12 @@ def test_workload_generator_deterministic():
 
 
 @pytest.mark.skipif(not have_ref(), reason="oracle/_ref not built (needs the reference sources)")
-def test_restatement_matches_live_reference(oracle):
+@pytest.mark.parametrize("n,order,k", [(24, 6, 30.0), (24, 4, 50 + 5j), (31, 2, 30 + 30j), (20, 6, 20 - 4j)])
+def test_restatement_matches_live_reference(oracle, n, order, k):
+    """The restatement against the reference's own C code built here, bit for bit, for real
+    and complex k."""
     from oracle import Reference2D
-    n, order, k = 24, 6, 30.0
-    f = W.source_2d(n, W.sine_modes(77, 8, 10), noise_seed=78, noise_var=1e-3)
+    f = W.source_2d(n, W.sine_modes(77 + n, 8, 10), noise_seed=78 + n, noise_var=1e-3)
     run = Reference2D().pipeline(n, order, k, f, threads=2)
     assert np.array_equal(oracle.pipeline_2d(n, order, k, f)["sol"], run.arrays["sol"].reshape(n, n))
 
