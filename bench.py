@@ -76,7 +76,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
@@ -121,75 +121,150 @@ class _quiet_stdout:
 
 
 def _reference_runner():
-    """(solve(f), kind, cores): the reference's own 2D C path (oracle/_ref, OpenMP over all host
-    cores) running coefficients() + rhs() + LU() + solver() on one right-hand side, as its main()
-    does; the oracle restatement (one core) where oracle/_ref was not built."""
+    """(solve(order, k, f_ext) -> u, kind, cores): the reference's own 2D C path (oracle/_ref,
+    OpenMP over all host cores) running coefficients() + rhs() + LU() + solver() on one
+    right-hand side, as its main() does; the oracle restatement (one core) where oracle/_ref was
+    not built."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    order, k = COMBOS[1]
     try:
         from oracle import Reference2D
         ref = Reference2D()
 
-        def solve(f):
+        def solve(order, k, f):
             with _quiet_stdout():
-                ref.pipeline(N, order, k, f, threads=cores)
+                run = ref.pipeline(N, order, k, f, threads=cores)
+            return run.arrays["sol"].reshape(N, N)
         return solve, "reference", cores
     except Exception:
         from oracle import Oracle
         orc = Oracle()
-        return (lambda f: orc.pipeline_2d(N, order, k, f)), "port", 1
+        return (lambda order, k, f: orc.pipeline_2d(N, order, k, f)["sol"]), "port", 1
 
 
-def _baseline_source(i: int):
+def _baseline_modes(i: int):
+    from hackathon_b200 import workload as W
+    return W.sine_modes(1000 + i, N_MODES, PMAX)
+
+
+def _baseline_source(i: int, noise: bool = True):
     from hackathon_b200 import workload as W
     seed = 1000 + i
-    return W.source_2d(N, W.sine_modes(seed, N_MODES, PMAX), noise_seed=seed + 0x1000000, noise_var=NOISE,
-                       fast=True)
+    return W.source_2d(N, _baseline_modes(i), noise_seed=seed + 0x1000000 if noise else None,
+                       noise_var=NOISE if noise else 0.0, fast=True)
 
 
 def _sample_text(done: int, kind: str) -> str:
-    order, k = COMBOS[1]
-    return (f"{done} RHS of 2D N=1023 order {order} k={k:g}: coefficients+rhs+LU+solver per RHS "
+    return (f"{done} RHS of 2D N=1023, one per (order, k) in {{4,6}} x {{10,50,200}} in turn: "
+            f"coefficients+rhs+LU+solver per RHS "
             f"({'reference C + project FFT shim; FFTW unavailable on this box' if kind == 'reference' else 'oracle port'})")
 
 
-def cpu_baseline(max_seconds: float = 25.0, max_rhs: int = 8) -> dict:
-    """Bounded sample of the reference CPU path on this host (source generation not timed)."""
+def cpu_baseline(gpu_solve=None, max_seconds: float = 25.0, max_rhs: int = 12) -> dict:
+    """Bounded sample of the reference CPU path on this host, cycling through the benchmark's six
+    (order, k) plans (source generation not timed).  With gpu_solve(order, k, f_interior) -> u
+    it is also the accuracy check of the benchmarked solve: the first right-hand side of every
+    (order, k) is compared with the reference's own output for it (max|u - u_ref| / max|u_ref|)."""
     solve, kind, cores = _reference_runner()
-    done, el = 0, 0.0
-    while done < max_rhs and el < max_seconds:
+    done, el, acc = 0, 0.0, {}
+    while done < max_rhs and (el < max_seconds or done < len(COMBOS)):
+        order, k = COMBOS[done % len(COMBOS)]
         f = _baseline_source(done)
         t0 = time.perf_counter()
-        solve(f)
+        u_ref = solve(order, k, f)
         el += time.perf_counter() - t0
+        if gpu_solve is not None and done < len(COMBOS):
+            u = gpu_solve(order, k, f[1:-1, 1:-1])
+            acc[f"o{order}_k{k:g}"] = float(np.abs(u - u_ref).max() / np.abs(u_ref).max())
         done += 1
-    return {"value": done / el, "unit": "solves/s", "cores": cores, "kind": kind, "sample": _sample_text(done, kind)}
+    out = {"value": done / el, "unit": "solves/s", "cores": cores, "kind": kind, "sample": _sample_text(done, kind)}
+    if acc:
+        out["rel_err_gpu_vs_cpu_reference"] = acc
+    return out
+
+
+def cpu_check_secondary() -> dict:
+    """CPU-baseline leg for the secondary configurations, one right-hand side each: the 3D
+    N=255 order-6 k=30 solve through the oracle restatement (one core: the reference's 3D CPU path
+    has no threads) and the 2D N=2047 order-6 k=400 solve through the reference's own C path
+    (all cores), each timed and compared with the GPU's solution of the same right-hand side."""
+    from hackathon_b200 import workload as W
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    out = {}
+    if "3d_n255_o6_k30_b4" in FIRST_RHS:
+        from oracle import Oracle
+        f = W.source_3d(255, W.sine_modes(2000, 16, 64, dim=3))
+        t0 = time.perf_counter()
+        ref = Oracle().pipeline_3d(255, 6, 30.0, f)["sol"]
+        dt = time.perf_counter() - t0
+        u = FIRST_RHS["3d_n255_o6_k30_b4"][30.0]
+        out["3d_n255_o6_k30"] = {"cpu_seconds_per_solve": dt, "cores": 1, "kind": "port",
+                                 "rel_err_gpu_vs_oracle": float(np.abs(u - ref).max() / np.abs(ref).max())}
+    if "2d_n2047_o6_b16" in FIRST_RHS:
+        cores = os.cpu_count() or 1
+        f = W.source_2d(2047, W.sine_modes(3000, 8, 20), fast=True)
+        try:
+            from oracle import Reference2D
+            ref2 = Reference2D()
+            t0 = time.perf_counter()
+            with _quiet_stdout():
+                run = ref2.pipeline(2047, 6, 400.0, f, threads=cores)
+            dt, kind = time.perf_counter() - t0, "reference"
+            ref = run.arrays["sol"].reshape(2047, 2047)
+        except Exception:
+            from oracle import Oracle
+            t0 = time.perf_counter()
+            ref = Oracle().pipeline_2d(2047, 6, 400.0, f)["sol"]
+            dt, kind, cores = time.perf_counter() - t0, "port", 1
+        u = FIRST_RHS["2d_n2047_o6_b16"][400.0]
+        out["2d_n2047_o6_k400"] = {"cpu_seconds_per_solve": dt, "cores": cores, "kind": kind,
+                                   "rel_err_gpu_vs_oracle": float(np.abs(u - ref).max() / np.abs(ref).max())}
+    return out
+
+
+def accuracy_vs_exact(gpu_solve) -> dict:
+    """Error of the benchmarked solve against the manufactured exact solution: the first
+    right-hand side of every (order, k) without its noise term (the noise has no closed-form
+    solution), max|u - u_exact| / max|u_exact|; the discretisation error of the scheme."""
+    from hackathon_b200 import workload as W
+    out = {}
+    for i, (order, k) in enumerate(COMBOS):
+        f = _baseline_source(i, noise=False)
+        u = gpu_solve(order, k, f[1:-1, 1:-1])
+        ex = W.exact_2d(N, _baseline_modes(i), k)
+        out[f"o{order}_k{k:g}"] = float(np.abs(u - ex).max() / np.abs(ex).max())
+    return out
 
 
 def run_reference(args, rank: int) -> None:
-    """The reference arm: each step is one right-hand side through the reference's CPU path."""
+    """The reference arm: each step is one right-hand side through the reference's CPU path,
+    cycling through the same six (order, k) plans as the GPU arm."""
     if rank != 0:
         return
     solve, kind, cores = _reference_runner()
-    srcs = [_baseline_source(i) for i in range(2)]
+    srcs = [_baseline_source(i) for i in range(len(COMBOS))]
     times = []
     for s in range(args.warmup + args.steps):
+        order, k = COMBOS[s % len(COMBOS)]
         t0 = time.perf_counter()
-        solve(srcs[s % 2])
+        solve(order, k, srcs[s % len(COMBOS)])
         times.append(time.perf_counter() - t0)
     timed = times[args.warmup:] or times[-1:]
     v = len(timed) / sum(timed)
     line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sine modes + CN(0,1e-3) noise)",
-            "config": {"workload": WORKLOAD, "n": N, "batch_per_step": 1, "order": COMBOS[1][0], "k": COMBOS[1][1]},
+            "config": {"workload": WORKLOAD, "n": N, "batch_per_step": 1, "orders": [4, 6], "k": [10, 50, 200],
+                       "form": "plain FP64", "fft": "project FFTW-API shim (FFTW is not installed on this box)"},
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": kind,
                              "sample": _sample_text(len(timed), kind)},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+FIRST_RHS: dict = {}  # secondary configuration -> {k: solution of its first right-hand side}
 
 
 def secondary_configs(hh, ctx, st, torch) -> dict:
@@ -233,7 +308,19 @@ def secondary_configs(hh, ctx, st, torch) -> dict:
         out[name] = {"solves_per_s": batch / (ms / 1000.0), "ms_per_step": ms,
                      "gpoints_per_s": pts / (ms / 1000.0) / 1e9,
                      "hbm_frac_of_96B_per_point": 96.0 * pts / (ms / 1000.0) / 1e9 / measured_hbm_peak()[0],
-                     "line_solve_variants": [p.variant for p in plans]}
+                     "line_solve_variants": [p.variant for p in plans], "rel_err_vs_exact": {}}
+        # accuracy of the first right-hand side of each plan's batch: against the manufactured
+        # exact solution here, against the oracle in the CPU-baseline leg (first_rhs)
+        first = {}
+        for p, g, k in zip(plans, graphs, ks):
+            g.replay()
+            torch.cuda.synchronize()
+            u0 = u[0].cpu().numpy()
+            ex = W.exact_3d(n, W.sine_modes(2000, 16, 64, dim=3), k) if dim == 3 else \
+                W.exact_2d(n, W.sine_modes(3000, 8, 20), k)
+            out[name]["rel_err_vs_exact"][f"k{k:g}"] = float(np.abs(u0 - ex).max() / np.abs(ex).max())
+            first[k] = u0
+        FIRST_RHS[name] = first
         del graphs
         for p in plans:
             p.close()
@@ -436,7 +523,15 @@ def main():
     t_wait = time.time()
     while not sampler.rows and time.time() - t_wait < 10:
         time.sleep(0.05)
+    # the clock record covers an untimed pre-roll of the same graph replays (0.5 s, so that even a
+    # short timed region has samples under the same load) and then the timed region itself
     sampler.rows.clear()
+    t_pre, s_pre = time.time(), 0
+    while time.time() - t_pre < 0.5:
+        graphs[s_pre % len(graphs)].replay()
+        s_pre += 1
+        if s_pre % 16 == 0:
+            torch.cuda.synchronize()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(st)
@@ -518,14 +613,25 @@ def main():
                     "d2h_bytes_per_step": io_bytes, "steps": e2e_steps},
             "gpu_launches": launches,
             "timing": "CUDA events on the launch stream around CUDA-graph replays (one graph per (order, k))",
-            "clocks": clk.summary(),
+            "clocks": dict(clk.summary(), window="0.5 s of the same graph replays just before the timed "
+                                                   "region, then the timed region (nvidia-smi every 20 ms)"),
         }
         if world == 1 and not args.no_secondary:
             line["secondary"] = secondary_configs(hh, ctx, st, torch)
             line["secondary"]["mixed_precision_refined"] = refined_configs(hh, ctx, st, torch)
             line["secondary"]["serving"] = serve_run(hh, torch, seconds=1.0)
+        def gpu_solve(order, k, f_int):
+            return plans[COMBOS.index((order, k))].solve_source_host(f_int)
+
+        line["accuracy"] = {"rel_err_vs_exact_noise_free_rhs": accuracy_vs_exact(gpu_solve)}
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline()
+            line["cpu_baseline"] = cpu_baseline(gpu_solve)
+            vs = line["cpu_baseline"].get("rel_err_gpu_vs_cpu_reference", {})
+            line["accuracy"]["rel_err_vs_cpu_reference"] = vs
+            line["accuracy"]["max_rel_err_vs_oracle"] = max(vs.values()) if vs else None
+            if "secondary" in line:
+                line["cpu_baseline"]["secondary"] = cpu_check_secondary()
+        line["accuracy"]["max_rel_err_vs_exact"] = max(line["accuracy"]["rel_err_vs_exact_noise_free_rhs"].values())
         print(json.dumps(line), flush=True)
     for p in plans:
         p.close()

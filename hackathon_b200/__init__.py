@@ -80,6 +80,7 @@ SIGNATURES = {
     "hh_server_stats": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(_sz), C.POINTER(_i)]),
     "hh_server_clock": (_d, [_vp]),
     "hh_server_destroy": (_i, [_vp]),
+    "hh_server_inject_error": (_i, [_vp, _i]),
 }
 
 _lib = None
@@ -264,9 +265,15 @@ class Plan:
         return mr.value, mf.value
 
     # -- host numpy arrays
+    def _batch_of(self, a: np.ndarray) -> int:
+        """Right-hand sides in `a`: a whole, non-zero number of fields, or HHError."""
+        if a.size == 0 or a.size % self.field:
+            raise HHError(f"array of {a.size} values is not a whole number of {self.field}-value fields")
+        return a.size // self.field
+
     def solve_host(self, rhs: np.ndarray) -> np.ndarray:
         rhs = np.ascontiguousarray(rhs, dtype=np.complex128)
-        batch = rhs.size // self.field
+        batch = self._batch_of(rhs)
         out = np.empty_like(rhs)
         check(lib().hh_solve_host(self.h, rhs.ctypes.data, out.ctypes.data, batch), "hh_solve_host")
         return out
@@ -274,7 +281,7 @@ class Plan:
     def solve_source_host_noalloc(self, f: np.ndarray) -> np.ndarray:
         """hh_solve_source_host_noalloc: staging in the library's fixed 32 MiB device array."""
         f = np.ascontiguousarray(f, dtype=np.complex128)
-        batch = f.size // self.field
+        batch = self._batch_of(f)
         out = np.empty_like(f)
         check(lib().hh_solve_source_host_noalloc(self.h, f.ctypes.data, out.ctypes.data, batch),
               "hh_solve_source_host_noalloc")
@@ -282,7 +289,7 @@ class Plan:
 
     def solve_source_host(self, f: np.ndarray) -> np.ndarray:
         f = np.ascontiguousarray(f, dtype=np.complex128)
-        batch = f.size // self.field
+        batch = self._batch_of(f)
         out = np.empty_like(f)
         check(lib().hh_solve_source_host(self.h, f.ctypes.data, out.ctypes.data, batch), "hh_solve_source_host")
         return out
@@ -333,6 +340,10 @@ class Server:
 
     def clock(self) -> float:
         return float(lib().hh_server_clock(self.h))
+
+    def inject_error(self, batches: int = 1):
+        """The next `batches` batches complete with HH_ERR_DEVICE (hh_server_inject_error)."""
+        check(lib().hh_server_inject_error(self.h, batches), "hh_server_inject_error")
 
     def close(self):
         if self.h:

@@ -20,8 +20,18 @@
 #include <mutex>
 #include <string>
 
+// Device staging for hh_solve_source_host_noalloc: one file-scope array per device, 32 MiB
+// (2^21 complex values: e.g. two 1023^2 right-hand sides or one 127^3).  Nothing in it has to
+// start at zero: every call writes each element it reads.  Calls that overlap in time on one
+// device share it and race; they must be serialized.
+constexpr long kNoAllocElems = 1L << 21;
+static __device__ __align__(256) double2 g_noalloc_stage[kNoAllocElems];
+
 struct hh_ctx {
     hh::Ctx c;
+    // device address of g_noalloc_stage on the context's device, looked up when the context is
+    // created (that lookup also loads this file's device code, so a later call allocates nothing)
+    double2 *noalloc_stage = nullptr;
     // device staging for hh_solve_host / hh_solve_source_host, shared by the context's plans
     // (host-buffer solves are synchronous, so one call uses it at a time)
     double2 *stage = nullptr;
@@ -97,6 +107,7 @@ extern "C" int hh_ctx_create(int device, void *stream, hh_ctx **out) {
     }
     cudaError_t e = cudaMalloc(&x->c.err_word, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(x->c.err_word, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaGetSymbolAddress((void **)&x->noalloc_stage, g_noalloc_stage);
     if (e != cudaSuccess) {
         if (x->c.own_stream) cudaStreamDestroy(x->c.stream);
         delete x;
@@ -807,12 +818,6 @@ extern "C" int hh_solve_source_host(hh_plan *pl, const double *f, double *u, int
 }
 
 // ------------------------------------------------------ allocation-free host solve ------
-// Device staging for hh_solve_source_host_noalloc: one file-scope array per device, 32 MiB
-// (2^21 complex values: e.g. two 1023^2 right-hand sides or one 127^3).  Nothing in it has to
-// start at zero: every call writes each element it reads.  Calls that overlap in time on one
-// device share it and race; they must be serialized.
-constexpr long kNoAllocElems = 1L << 21;
-static __device__ __align__(256) double2 g_noalloc_stage[kNoAllocElems];
 
 extern "C" int hh_solve_source_host_noalloc(hh_plan *pl, const double *f_host, double *u_host, int batch) {
     HH_TRY(check_batch(pl, batch));
@@ -830,16 +835,8 @@ extern "C" int hh_solve_source_host_noalloc(hh_plan *pl, const double *f_host, d
     }
     Ctx *c = p.ctx;
     HH_CUDA(cudaSetDevice(c->device));
-    // the staging address, looked up once per device
-    static std::mutex mu;
-    static double2   *addr[64] = {};
-    double2          *d = nullptr;
-    {
-        std::lock_guard<std::mutex> g(mu);
-        if (c->device < 0 || c->device >= 64) { set_error("device %d", c->device); return HH_ERR_INVALID; }
-        if (!addr[c->device]) HH_CUDA(cudaGetSymbolAddress((void **)&addr[c->device], g_noalloc_stage));
-        d = addr[c->device];
-    }
+    // the array's address on this device, looked up when the context was created
+    double2 *d = reinterpret_cast<hh_ctx *>(c)->noalloc_stage; // Ctx is the first member of hh_ctx
     const size_t bytes = sizeof(double2) * (size_t)p.field * batch;
     HH_CUDA(cudaMemcpyAsync(d, f_host, bytes, cudaMemcpyHostToDevice, c->stream));
     HH_TRY(hh_solve_source(pl, (const double *)d, (double *)d, batch));

@@ -65,6 +65,11 @@ struct hh_server {
     cudaEvent_t                         ready = nullptr;   // set-up done, per plan creation
     cudaMemPool_t                       pool = nullptr;
     int                                *flags = nullptr; // pinned, one slot per stream
+    // device error words, one per stream: a batch clears its stream's word first and copies it to
+    // its flag slot last, so an expired wait fails only the batch whose kernel reported it
+    int                                *words = nullptr;
+    int                                *own_word = nullptr; // the context's own word (restored at exit)
+    int                                 inject = 0;         // batches still to fail (hh_server_inject_error)
     size_t                              budget = 0, used = 0;
     std::mutex                          m;
     std::condition_variable             cv;
@@ -176,8 +181,19 @@ int run_batch(hh_server *s, Batch *b, hh_plan *plan, cudaEvent_t after) {
     const int         si = s->rr++ % (int)s->streams.size();
     cudaStream_t      st = s->streams[(size_t)si];
     double2          *buf = nullptr;
+    hh::Ctx          *cx = reinterpret_cast<hh::Ctx *>(s->ctx); // Ctx is hh_ctx's first member
+    bool              inject = false;
+    {
+        std::lock_guard<std::mutex> g(s->m);
+        if (s->inject > 0) {
+            s->inject--;
+            inject = true;
+        }
+    }
     auto enqueue = [&]() -> int {
         HH_TRY(hh_ctx_set_stream(s->ctx, st));
+        cx->err_word = s->words + si; // the kernels of this batch report into its stream's word
+        HH_CUDA(cudaMemsetAsync(cx->err_word, 0, sizeof(int), st));
         if (after) HH_CUDA(cudaStreamWaitEvent(st, after, 0)); // the plan's set-up
         int total = 0;
         for (Req *q : b->reqs) total += q->r.nrhs;
@@ -203,9 +219,9 @@ int run_batch(hh_server *s, Batch *b, hh_plan *plan, cudaEvent_t after) {
             HH_CUDA(cudaFreeAsync(buf, st));
             buf = nullptr;
         }
+        if (inject) HH_CUDA(cudaMemsetAsync(cx->err_word, 1, 1, st)); // as if a wait had expired
         b->flag = s->flags + si;
-        HH_CUDA(cudaMemcpyAsync(b->flag, reinterpret_cast<hh::Ctx *>(s->ctx)->err_word, sizeof(int),
-                                cudaMemcpyDeviceToHost, st));
+        HH_CUDA(cudaMemcpyAsync(b->flag, cx->err_word, sizeof(int), cudaMemcpyDeviceToHost, st));
         HH_CUDA(cudaLaunchHostFunc(st, batch_done, b));
         return HH_OK;
     };
@@ -343,6 +359,9 @@ extern "C" int hh_server_create(int device, size_t budget, int streams, hh_serve
     }
     if (e == cudaSuccess) e = cudaHostAlloc((void **)&s->flags, sizeof(int) * 64, cudaHostAllocDefault);
     if (e == cudaSuccess) memset(s->flags, 0, sizeof(int) * 64);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&s->words, sizeof(int) * 64);
+    if (e == cudaSuccess) e = cudaMemset(s->words, 0, sizeof(int) * 64);
+    if (e == cudaSuccess) s->own_word = reinterpret_cast<hh::Ctx *>(s->ctx)->err_word;
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->setup, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ready, cudaEventDisableTiming);
     if (e == cudaSuccess) reinterpret_cast<hh::Ctx *>(s->ctx)->pool = s->pool;
@@ -356,6 +375,7 @@ extern "C" int hh_server_create(int device, size_t budget, int streams, hh_serve
         for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
         if (s->pool) cudaMemPoolDestroy(s->pool);
         if (s->flags) cudaFreeHost(s->flags);
+        if (s->words) cudaFree(s->words);
         hh_ctx_destroy(s->ctx);
         delete s;
         return HH_ERR_CUDA;
@@ -435,12 +455,24 @@ extern "C" int hh_server_destroy(hh_server *s) {
     for (auto &kv : s->plans) hh_plan_destroy(kv.second.plan);
     for (auto &kv : s->reqs) delete kv.second;
     cudaStreamSynchronize(s->setup);
+    reinterpret_cast<hh::Ctx *>(s->ctx)->err_word = s->own_word; // the context frees its own word
     hh_ctx_destroy(s->ctx); // while its current stream (one of the server's) still exists
     for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
     cudaStreamDestroy(s->setup);
     cudaEventDestroy(s->ready);
     cudaMemPoolDestroy(s->pool);
     cudaFreeHost(s->flags);
+    cudaFree(s->words);
     delete s;
+    return HH_OK;
+}
+
+extern "C" int hh_server_inject_error(hh_server *s, int batches) {
+    if (!s || batches < 0) {
+        set_error("hh_server_inject_error: invalid arguments");
+        return HH_ERR_INVALID;
+    }
+    std::lock_guard<std::mutex> g(s->m);
+    s->inject = batches;
     return HH_OK;
 }

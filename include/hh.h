@@ -132,9 +132,11 @@ int hh_solve_source_host(hh_plan *plan, const double *f_host, double *u_host, in
  * callers that must not allocate device memory while they run, e.g. with a fixed memory budget
  * or where allocator latency is unwelcome: the device staging is a 32 MiB array of the library
  * (2^21 complex values, so field size * batch <= 2097152, e.g. two 1023^2 or one 127^3
- * right-hand sides; larger requests fail with HH_ERR_UNSUPPORTED).  The first call on a device
- * looks up the array's address; make it before any stream capture.  The array is shared by all
- * contexts on a device: calls that overlap in time race and must be serialized by the caller. */
+ * right-hand sides; larger requests fail with HH_ERR_UNSUPPORTED).  hh_ctx_create looks up the
+ * array's address on its device (this also loads the library's device code), so no call of this
+ * function allocates, its first call on a new context included; a context must not outlive a
+ * reset of its device.  The array is shared by all contexts on a device: calls that overlap in
+ * time race and must be serialized by the caller. */
 int hh_solve_source_host_noalloc(hh_plan *plan, const double *f_host, double *u_host, int batch);
 
 /* FP64 residual res = A_h sol - rhs of the plan's compact operator for `batch` fields on the
@@ -196,6 +198,12 @@ int    hh_server_wait(hh_server *s, long long id, hh_request_info *info); /* blo
 int    hh_server_stats(hh_server *s, long long *completed, size_t *bytes_in_use, int *plans);
 double hh_server_clock(hh_server *s);
 int    hh_server_destroy(hh_server *s); /* finishes every submitted request first */
+/* Host-side failure injection (no counterpart in the reference, which only prints CUDA errors,
+ * 3D_Program/solver_functions/cuda_helper.h:33-48): the next `batches` batches the loop starts
+ * run their solves unchanged but complete with HH_ERR_DEVICE, exactly as if one of their kernels
+ * had reported an expired bounded wait.  Each stream has its own device error word, cleared
+ * before every batch, so a failure is charged to its own batch only and later batches succeed. */
+int    hh_server_inject_error(hh_server *s, int batches);
 
 #ifdef __cplusplus
 }

@@ -11,7 +11,10 @@
  * The struct types below reproduce 2D_Program/headers/structs.h:12-30 field for field (same
  * sizes and offsets, 192-byte System) under hh2d_ names so this header can be included next
  * to the reference's own.  The FFTW plan/buffer arguments of forwardDST/reverseDST are
- * accepted and ignored (declared as void *, ABI-identical to the reference's pointer types).
+ * accepted and ignored (declared as void *, ABI-identical to the reference's pointer types);
+ * dst.Nx (transform length, 1..sys.lat.Nx) and dst.coef (output scale) are honoured as in
+ * DST.c:15-21,35-40.  Device and host staging are kept between calls, so a loop of calls does not
+ * allocate per call.
  *
  * Semantics: solver() reads sys.rhs and the stencil rows sys.bp..sys.am, rebuilds the shifted
  * Thomas factors on the GPU (the values LU() leaves in sys.L/U/Up are not read), and writes

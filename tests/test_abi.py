@@ -48,18 +48,16 @@ def test_dropin_libraries_export_reference_entry_points(header, lib, expect):
     C.CDLL(lib)  # loads (and pulls libhh.so through its rpath)
 
 
-def _compile_run(src: str) -> str:
-    d = os.path.join(ROOT, "_work")
-    os.makedirs(d, exist_ok=True)
-    c = os.path.join(d, "abi_probe.c")
-    exe = os.path.join(d, "abi_probe")
+def _compile_run(src: str, d) -> str:
+    c = os.path.join(str(d), "abi_probe.c")
+    exe = os.path.join(str(d), "abi_probe")
     open(c, "w").write(src)
     r = subprocess.run(["/usr/bin/gcc", "-I", INCLUDE, c, "-o", exe], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     return subprocess.run([exe], capture_output=True, text=True).stdout
 
 
-def test_dropin_struct_layouts_match_reference():
+def test_dropin_struct_layouts_match_reference(tmp_path):
     """192-byte 2D System / 312-byte 3D System with the reference's field offsets
     (2D_Program/headers/structs.h:20-30, 3D_Program/headers/structs.h:46-58)."""
     out = _compile_run(textwrap.dedent("""
@@ -72,7 +70,7 @@ def test_dropin_struct_layouts_match_reference():
                    offsetof(hh2d_System, order), offsetof(hh2d_System, k), offsetof(hh2d_System, am));
             printf("%zu\\n", sizeof(hh2d_DSTN));
             return 0;
-        }"""))
+        }"""), tmp_path)
     assert out.split() == ["192", "64", "68", "72", "184", "16"]
     out3 = _compile_run(textwrap.dedent("""
         #include <stdio.h>
@@ -83,7 +81,7 @@ def test_dropin_struct_layouts_match_reference():
                    offsetof(hh3d_System, order), offsetof(hh3d_System, a), offsetof(hh3d_System, A),
                    offsetof(hh3d_System, sol), offsetof(hh3d_System, error));
             return 0;
-        }"""))
+        }"""), tmp_path)
     assert out3.split() == ["312", "88", "88", "96", "208", "288", "304"]
 
 
@@ -123,3 +121,4 @@ def test_invalid_arguments_are_rejected_without_a_gpu():
     assert L.hh_dst1_rows(None, 7, 1, None, 7, None, 7) == 1
     assert L.hh_solve(None, None, None, 1) == 1
     assert b"invalid" in L.hh_last_error()
+    assert L.hh_server_inject_error(None, 1) == 1

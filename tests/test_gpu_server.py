@@ -96,3 +96,27 @@ def test_budget_admission_and_rejection(ctx):
     srv.wait(ok)
     srv.close()
     assert np.array_equal(outs[0].numpy(), _solo(ctx, 2, n, 6, 10.0, f))
+
+
+def test_injected_failure_fails_only_its_batch(ctx):
+    """A batch whose error word is set (host-side injection, as if one of its kernels had seen a
+    bounded wait expire) fails with HH_ERR_DEVICE; the batches after it, on the same stream and
+    on the others, succeed with the solo result: every stream's word is cleared per batch."""
+    n, nrhs = 63, 2
+    rng = np.random.default_rng(9)
+    f = rng.standard_normal((nrhs, n, n)) + 1j * rng.standard_normal((nrhs, n, n))
+    solo = _solo(ctx, 2, n, 4, 7.0, f)
+    srv = hh.Server(0, hbm_budget=2 << 30, streams=2)
+    fp = torch.from_numpy(f).pin_memory()
+    outs = [torch.empty_like(fp).pin_memory() for _ in range(5)]
+    first = srv.submit(2, n, 4, 7.0, nrhs, fp, outs[0])
+    srv.wait(first)  # the plan exists; the next request runs alone
+    srv.inject_error(1)
+    bad = srv.submit(2, n, 4, 7.0, nrhs, fp, outs[1])
+    with pytest.raises(hh.HHError, match="HH_ERR_DEVICE"):
+        srv.wait(bad)
+    for i in range(2, 5):  # both streams, round robin: each succeeds
+        srv.wait(srv.submit(2, n, 4, 7.0, nrhs, fp, outs[i]))
+    srv.close()
+    for i in (0, 2, 3, 4):
+        assert np.array_equal(outs[i].numpy(), solo)

@@ -37,15 +37,29 @@ def test_noalloc_3d_and_rejection(ctx):
     big.close()
 
 
+def _free_bytes():
+    import torch
+    torch.cuda.synchronize()
+    return torch.cuda.mem_get_info(0)[0]
+
+
 def test_noalloc_first_call_on_a_fresh_context():
     """The allocation-free call as the very first solve of a new context (every table it needs
-    was made when the plan was created), then again, against the allocating entry point."""
+    was made when the plan was created), then again, against the allocating entry point.  The
+    device's free memory is the same before and after each of the two calls: neither call
+    allocates, the first included."""
+    pytest.importorskip("torch")
+    _free_bytes()  # the runtime's own first-use set-up happens here, outside the checks
     ctx = hh.Context(0)
     n = 1023
     plan = hh.Plan.helmholtz(ctx, 2, n, 4, 30.0)
     f1, f2 = _f(n, 7), _f(n, 8)
+    before = _free_bytes()
     got1 = plan.solve_source_host_noalloc(f1)
+    after1 = _free_bytes()
     got2 = plan.solve_source_host_noalloc(f2)
+    after2 = _free_bytes()
+    assert before == after1 == after2, (before, after1, after2)
     assert np.array_equal(got1, plan.solve_source_host(f1))
     assert np.array_equal(got2, plan.solve_source_host(f2))
     plan.close()
