@@ -63,6 +63,10 @@ SIGNATURES = {
     "hh_plan_tune": (_i, [_vp, _i]),
     "hh_plan_set_variant": (_i, [_vp, _i]),
     "hh_plan_variant": (_i, [_vp]),
+    "hh_plan_set_slab": (_i, [_vp, _l]),
+    "hh_plan_slab": (_l, [_vp]),
+    "hh_plan_set_dst_variant": (_i, [_vp, _i]),
+    "hh_plan_dst_variant": (_i, [_vp]),
     "hh_solve": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_host": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source": (_i, [_vp, _vp, _vp, _i]),
@@ -239,6 +243,24 @@ class Plan:
     @variant.setter
     def variant(self, v: int):
         check(lib().hh_plan_set_variant(self.h, v), "hh_plan_set_variant")
+
+    @property
+    def slab(self) -> int:
+        """3D: planes per slab of the transform passes (0: the whole batch)."""
+        return int(lib().hh_plan_slab(self.h))
+
+    @slab.setter
+    def slab(self, planes: int):
+        check(lib().hh_plan_set_slab(self.h, planes), "hh_plan_set_slab")
+
+    @property
+    def dst_variant(self) -> int:
+        """3D: the column-transform kernel (0: CTA tiles of 8 swizzled columns, 1: per-warp tiles)."""
+        return int(lib().hh_plan_dst_variant(self.h))
+
+    @dst_variant.setter
+    def dst_variant(self, v: int):
+        check(lib().hh_plan_set_dst_variant(self.h, v), "hh_plan_set_dst_variant")
 
     # -- device buffers (torch tensors / raw addresses)
     def solve(self, rhs, sol, batch: int = 1):

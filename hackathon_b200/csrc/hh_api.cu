@@ -96,8 +96,11 @@ extern "C" int hh_ctx_create(int device, void *stream, hh_ctx **out) {
     HH_CUDA(cudaGetDeviceCount(&ndev));
     if (device < 0 || device >= ndev) { set_error("hh_ctx_create: device %d of %d", device, ndev); return HH_ERR_INVALID; }
     HH_CUDA(cudaSetDevice(device));
+    int l2 = 0;
+    HH_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device));
     hh_ctx *x = new hh_ctx();
     x->c.device = device;
+    x->c.l2_bytes = l2 > 0 ? (size_t)l2 : (size_t)(50u << 20);
     if (stream) {
         x->c.stream = (cudaStream_t)stream;
     } else {
@@ -547,6 +550,9 @@ extern "C" int hh_plan_set_variant(hh_plan *pl, int variant) {
 
 extern "C" int hh_plan_variant(const hh_plan *pl) { return pl ? pl->p.variant : -1; }
 
+static int transform_forward(Plan &p, const double2 *in, double2 *out, int batch, bool lp = false);
+static int transform_inverse(Plan &p, double2 *buf, int batch, bool lp = false);
+
 // Times every line-solve variant on `batch` zero right-hand sides (the solve does the same work
 // for any values) and keeps the fastest.  Blocks; must not run inside a stream capture.
 extern "C" int hh_plan_tune(hh_plan *pl, int batch) {
@@ -585,6 +591,45 @@ extern "C" int hh_plan_tune(hh_plan *pl, int batch) {
     };
     rc = run();
     p.variant = best;
+    // 3D plans: the slab of the transform passes, over candidates from a sixteenth of L2 to the
+    // whole batch, timed as one forward and one inverse transform
+    if (rc == HH_OK && p.dim == 3) {
+        const long planes = (long)p.nz * batch, plane_bytes = 16L * p.nx * p.ny;
+        std::vector<long> cand = {planes};
+        for (long div : {16L, 8L, 4L, 3L, 2L}) {
+            const long sp = std::max(1L, (long)(c->l2_bytes / div) / plane_bytes);
+            if (sp < planes && std::find(cand.begin(), cand.end(), sp) == cand.end()) cand.push_back(sp);
+        }
+        long  best_slab = p.slab;
+        int   best_ck = p.col_kernel;
+        float best_t = 1e30f;
+        for (int trial = 0; trial < 2 * (int)cand.size(); trial++) {
+            const long sp = cand[(size_t)trial / 2];
+            p.slab = sp;
+            p.col_kernel = trial % 2;
+            auto pass = [&]() -> int {
+                HH_TRY(transform_forward(p, buf, buf, batch));
+                return transform_inverse(p, buf, batch);
+            };
+            if ((rc = pass()) != HH_OK) break;
+            if (cudaEventRecord(e0, c->stream) != cudaSuccess) { rc = HH_ERR_CUDA; break; }
+            for (int r = 0; r < 3 && rc == HH_OK; r++) rc = pass();
+            if (rc != HH_OK) break;
+            float ms = 0.f;
+            if (cudaEventRecord(e1, c->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+                rc = HH_ERR_CUDA;
+                break;
+            }
+            if (ms < best_t) {
+                best_t = ms;
+                best_slab = sp;
+                best_ck = p.col_kernel;
+            }
+        }
+        p.slab = best_slab;
+        p.col_kernel = best_ck;
+    }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (buf) {
@@ -596,29 +641,65 @@ extern "C" int hh_plan_tune(hh_plan *pl, int batch) {
 }
 
 // -------------------------------------------------------------------- solve ------
+// 3D transforms can run slab by slab: the rows pass over a slab of planes, then the columns
+// pass over the same slab, which then finds the rows pass's output in L2, so that a value crosses
+// HBM once per direction instead of twice (the reference's per-plane DST(),
+// 3D_Program/solver_functions/DST.c:148-204 inside solver.c:338-350, makes both passes over one
+// plane at a time in host memory).  Measured at 255^3 x 4: both passes are bound by latency, not
+// by HBM, so the extra launches cost more than the saved traffic (2.73 ms per solve over the
+// whole batch, 2.82 ms with slabs of 128 planes, 5.34 ms with 8); the default is therefore the
+// whole batch in one slab, and hh_plan_tune keeps a smaller slab only where it measures faster.
+long hh::slab_planes(const Plan &p, long planes) {
+    const long s = p.slab > 0 ? p.slab : planes;
+    return std::max(1L, std::min(std::min(s, planes), 65535L));
+}
+
 // lp: single-precision transform arithmetic (the refined solve's low-precision solves)
-static int transform_forward(Plan &p, const double2 *in, double2 *out, int batch, bool lp = false) {
+static int transform_forward(Plan &p, const double2 *in, double2 *out, int batch, bool lp) {
     Ctx *c = p.ctx;
     if (p.dim == 2) return launch_dst_rows(c, p.nx, (long)p.ny * batch, in, p.nx, out, p.nx, lp);
-    const long plane = (long)p.nx * p.ny, planes = (long)p.nz * batch;
-    HH_TRY(launch_dst_rows(c, p.nx, (long)p.ny * planes, in, p.nx, out, p.nx, lp));
-    for (long p0 = 0; p0 < planes; p0 += 65535) {
-        const long np = (planes - p0 < 65535) ? planes - p0 : 65535;
-        HH_TRY(launch_dst_cols(c, p.ny, p.nx, np, out + p0 * plane, p.nx, plane, out + p0 * plane, lp));
+    const long plane = (long)p.nx * p.ny, planes = (long)p.nz * batch, sp = slab_planes(p, planes);
+    for (long p0 = 0; p0 < planes; p0 += sp) {
+        const long np = std::min(sp, planes - p0);
+        HH_TRY(launch_dst_rows(c, p.nx, (long)p.ny * np, in + p0 * plane, p.nx, out + p0 * plane, p.nx, lp));
+        HH_TRY(launch_dst_cols(c, p.ny, p.nx, np, out + p0 * plane, p.nx, plane, out + p0 * plane, lp, p.col_kernel));
     }
     return HH_OK;
 }
 
-static int transform_inverse(Plan &p, double2 *buf, int batch, bool lp = false) {
+static int transform_inverse(Plan &p, double2 *buf, int batch, bool lp) {
     Ctx *c = p.ctx;
     if (p.dim == 2) return launch_dst_rows(c, p.nx, (long)p.ny * batch, buf, p.nx, buf, p.nx, lp);
-    const long plane = (long)p.nx * p.ny, planes = (long)p.nz * batch;
-    for (long p0 = 0; p0 < planes; p0 += 65535) {
-        const long np = (planes - p0 < 65535) ? planes - p0 : 65535;
-        HH_TRY(launch_dst_cols(c, p.ny, p.nx, np, buf + p0 * plane, p.nx, plane, buf + p0 * plane, lp));
+    const long plane = (long)p.nx * p.ny, planes = (long)p.nz * batch, sp = slab_planes(p, planes);
+    for (long p0 = 0; p0 < planes; p0 += sp) {
+        const long np = std::min(sp, planes - p0);
+        HH_TRY(launch_dst_cols(c, p.ny, p.nx, np, buf + p0 * plane, p.nx, plane, buf + p0 * plane, lp, p.col_kernel));
+        HH_TRY(launch_dst_rows(c, p.nx, (long)p.ny * np, buf + p0 * plane, p.nx, buf + p0 * plane, p.nx, lp));
     }
-    return launch_dst_rows(c, p.nx, (long)p.ny * planes, buf, p.nx, buf, p.nx, lp);
+    return HH_OK;
 }
+
+extern "C" int hh_plan_set_slab(hh_plan *pl, long planes) {
+    if (!pl || planes < 0) {
+        set_error("hh_plan_set_slab: invalid plan or slab (%ld)", planes);
+        return HH_ERR_INVALID;
+    }
+    pl->p.slab = planes;
+    return HH_OK;
+}
+
+extern "C" long hh_plan_slab(const hh_plan *pl) { return pl ? pl->p.slab : -1; }
+
+extern "C" int hh_plan_set_dst_variant(hh_plan *pl, int v) {
+    if (!pl || v < 0 || v > 1) {
+        set_error("hh_plan_set_dst_variant: invalid plan or variant (%d)", v);
+        return HH_ERR_INVALID;
+    }
+    pl->p.col_kernel = v;
+    return HH_OK;
+}
+
+extern "C" int hh_plan_dst_variant(const hh_plan *pl) { return pl ? pl->p.col_kernel : -1; }
 
 static int check_batch(hh_plan *pl, int batch) {
     if (!pl || batch < 0 || batch > 65535) {

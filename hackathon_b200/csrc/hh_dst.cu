@@ -1044,6 +1044,117 @@ __global__ void __launch_bounds__(32 * WCfg<M>::CWPC, 3)
     }
 }
 
+// ---- columns, CTA tiles: TC = 8 neighbouring columns of all rows arrive as 128-byte-wide boxes of
+// a 3-D map (the doubles of a row, row, plane) with 128-byte swizzle, so that each row of a tile
+// is one 128-byte piece of global memory (instead of the LPW * 16 bytes of the per-warp tiles
+// above) and reading a column of the tile is free of bank conflicts: element (row r, column cc)
+// of a box sits at byte r * 128 + 16 * (cc ^ (r % 8)).  The CTA's WPC = TC / LPW warps each
+// transform LPW of the tile's columns (lanes line-major: lane = c * TL + l), write the outputs
+// back into the tile, and one thread stores the tile with tensor stores and refills the buffer
+// with the CTA's tile NT tickets ahead once the store has read it.
+template <int M> struct WTile {
+    using G = WGeom<M>;
+    static constexpr int TL = G::TL, LPW = G::LPW, N = M - 1;
+    static constexpr int TC = 8;                  // columns per tile: one 128-byte swizzle span
+    static constexpr int WPC = TC / LPW;          // warps per CTA
+    static constexpr int BR = N < 256 ? N : 256;  // rows per box
+    static constexpr int NBOX = (N + BR - 1) / BR;
+    static constexpr int BOX_BYTES = (BR * 128 + 1023) / 1024 * 1024; // boxes stay 1024-byte aligned
+    static constexpr int TILE_BYTES = NBOX * BOX_BYTES;
+    static constexpr int NT = 2;                  // tiles per CTA (one loads while one is used)
+    static constexpr int XBUF = (G::BUF + 7) / 8 * 8; // exchange area per line (elements)
+    static constexpr int SMEM = 1024 + NT * TILE_BYTES + 16 * TC * XBUF; // + alignment slack
+    static_assert(WPC * LPW == TC, "the warps cover the tile's columns");
+};
+
+template <int M, bool LP = false>
+__global__ void __launch_bounds__(32 * WTile<M>::WPC)
+    k_dst1_wt(const __grid_constant__ CUtensorMap in_map, const __grid_constant__ CUtensorMap out_map, long ncols,
+              long nplanes, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
+    using G = WGeom<M>;
+    using TG = WTile<M>;
+    constexpr int TL = G::TL, LPW = G::LPW, KB = G::KB, N = M - 1, K2 = 2 * KB;
+    constexpr int TC = TG::TC, BR = TG::BR, NBOX = TG::NBOX, NT = TG::NT;
+    __shared__ __align__(8) uint64_t full[NT];
+    extern __shared__ __align__(1024) unsigned char wt_raw[];
+    // 1024-byte aligned tiles (the 128-byte swizzle pattern repeats every 1024 bytes)
+    unsigned char *tiles = wt_raw + ((1024u - (smem_u32(wt_raw) & 1023u)) & 1023u);
+    const int      lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+    const int      c = lane / TL, l = lane % TL;
+    const int      col = wq * LPW + c; // this line's column within the tile
+    double2       *xbuf = reinterpret_cast<double2 *>(tiles + NT * TG::TILE_BYTES) + (long)col * TG::XBUF;
+    if ((smem_u32(tiles) & 1023u) != 0) { // cannot happen with the slack above; never issue a misaligned copy
+        if (threadIdx.x == 0) atomicExch(err, 2);
+        return;
+    }
+    const long cgroups = (ncols + TC - 1) / TC;
+    const long groups = cgroups * nplanes;
+    if ((long)blockIdx.x >= groups) return; // whole CTA
+    const int tickets = (int)((groups - blockIdx.x + gridDim.x - 1) / gridDim.x);
+    auto coords = [&](int t, int &x0, int &p) {
+        const long g = (long)blockIdx.x + (long)t * gridDim.x;
+        x0 = (int)(g % cgroups) * TC;
+        p = (int)(g / cgroups);
+    };
+    auto fetch = [&](int t) { // thread 0: ticket t into buffer t % NT
+        int x0, p;
+        coords(t, x0, p);
+        unsigned char *dst = tiles + (t % NT) * TG::TILE_BYTES;
+        mbar_expect_tx(&full[t % NT], (uint32_t)(NBOX * BR * 128));
+        for (int b = 0; b < NBOX; b++) tma_load_3d(dst + b * TG::BOX_BYTES, &in_map, 2 * x0, b * BR, p, &full[t % NT]);
+    };
+    if (threadIdx.x == 0) {
+        for (int u = 0; u < NT; u++) mbar_init(&full[u], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (int u = 0; u < NT && u < tickets; u++) fetch(u);
+    }
+    __syncthreads();
+    WConst<M> K;
+    K.load(l, tw, sn);
+
+    int failed = -1;
+    for (int t = 0; t < tickets; t++) {
+        const int s = t % NT;
+        // every thread waits (bounded); the CTA leaves together if any wait expired
+        const bool ok = mbar_wait_parity(&full[s], (uint32_t)((t / NT) & 1));
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicExch(err, 1);
+            failed = t;
+            break;
+        }
+        unsigned char *tile = tiles + s * TG::TILE_BYTES;
+        auto at = [&](int row) -> double2 * { // element (row, col) of the tile
+            const int b = row / BR, r = row - b * BR;
+            return reinterpret_cast<double2 *>(tile + b * TG::BOX_BYTES + r * 128 + ((col ^ (r & 7)) << 4));
+        };
+        int x0, p;
+        coords(t, x0, p);
+        const bool live = x0 + col < ncols;
+        if constexpr (LP) w_transform_lp<M, false>([&](int j) { return *at(j - 1); }, xbuf, l, live, K);
+        else w_transform<M, false>([&](int j) { return *at(j - 1); }, xbuf, l, live, K);
+#pragma unroll
+        for (int q = 0; q < M / TL; q++) {
+            const int pp = l + TL * q;
+            if (pp < N) *at(pp) = xbuf[(K2 + 1) * (pp / K2) + pp % K2];
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // tile writes before the store reads
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int b = 0; b < NBOX; b++) tma_store_3d(&out_map, 2 * x0, b * BR, p, tile + b * TG::BOX_BYTES);
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+            if (t + NT < tickets) {
+                asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); // the store has read the tile
+                fetch(t + NT);
+            }
+        }
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); // stores complete before exit
+        if (failed >= 0) // loads still in flight get a bounded chance to land
+            for (int u = failed; u < tickets && u < failed + NT; u++) mbar_wait_parity(&full[u % NT], (uint32_t)((u / NT) & 1));
+    }
+}
+
 // ---------------------------------------------- direct DST (any n, dense sine matrix) ----
 // out_k = sqrt(2/(n+1)) sum_m in_m sin(pi (k+1)(m+1)/(n+1)); `mat` holds the n*n sines.
 constexpr int kDenseThreads = 128;
@@ -1277,7 +1388,7 @@ static int encode_col_map(CUtensorMap *map, const double2 *base, long ncols, lon
 }
 
 int encode_tensor_map(CUtensorMap *map, const void *base, int rank, const unsigned long long *dims,
-                      const unsigned long long *strides, const unsigned *box) {
+                      const unsigned long long *strides, const unsigned *box, bool swizzle128) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
         cudaDriverEntryPointQueryResult q;
@@ -1297,7 +1408,8 @@ int encode_tensor_map(CUtensorMap *map, const void *base, int rank, const unsign
         if (i + 1 < rank) s[i] = strides[i];
     }
     const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (cuuint32_t)rank, const_cast<void *>(base), d, s, b, e,
-                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -1331,8 +1443,55 @@ static int launch_wc(Ctx *c, long ncols, long planes, const double2 *in, long ld
     return HH_OK;
 }
 
+// (double, row, plane) map of column tiles: boxes of 16 doubles (8 complex columns) by br rows,
+// 128-byte swizzle
+static int encode_tile_map(CUtensorMap *map, const double2 *base, long ncols, long rows, long planes, long ld,
+                           long plane_stride, int box_rows) {
+    const unsigned long long dims[3] = {2ULL * (unsigned long long)ncols, (unsigned long long)rows,
+                                        (unsigned long long)planes};
+    const unsigned long long strides[2] = {(unsigned long long)ld * 16, (unsigned long long)plane_stride * 16};
+    const unsigned           box[3] = {16, (unsigned)box_rows, 1};
+    return encode_tensor_map(map, base, 3, dims, strides, box, true);
+}
+
+template <int M>
+static int launch_wt(Ctx *c, long ncols, long planes, const double2 *in, long ld, long plane_stride, double2 *out,
+                     bool lp) {
+    using TG = WTile<M>;
+    const double2 *tw;
+    const double  *sn;
+    HH_TRY(tables_for(c, M, &tw, &sn));
+    CUtensorMap in_map, out_map;
+    HH_TRY(encode_tile_map(&in_map, in, ncols, M - 1, planes, ld, plane_stride, TG::BR));
+    HH_TRY(encode_tile_map(&out_map, out, ncols, M - 1, planes, ld, plane_stride, TG::BR));
+    auto kern = lp ? k_dst1_wt<M, true> : k_dst1_wt<M, false>;
+    HH_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, TG::SMEM));
+    int dev = 0, sms = 148, per_sm = 0;
+    HH_CUDA(cudaGetDevice(&dev));
+    HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * TG::WPC, TG::SMEM));
+    const long groups = (ncols + TG::TC - 1) / TG::TC * planes;
+    const long ctas = std::min<long>(groups, (long)std::max(1, per_sm) * sms);
+    kern<<<(unsigned)ctas, 32 * TG::WPC, TG::SMEM, c->stream>>>(in_map, out_map, ncols, planes, tw, sn, c->err_word);
+    HH_CUDA(cudaGetLastError());
+    c->launches++;
+    return HH_OK;
+}
+
 int launch_dst_cols(Ctx *c, int n, long ncols, long planes, const double2 *in, long ld, long plane_stride,
-                    double2 *out, bool lp) {
+                    double2 *out, bool lp, int kern) {
+    // CTA tiles of 8 swizzled columns: the tensor map covers 2 * ncols doubles per row (an
+    // 8-column box needs ncols >= 8), rows ld * 16 and planes plane_stride * 16 bytes apart
+    if (kern == 0 && planes > 0 && ncols >= 8 && ld * 16 < (1L << 40) && plane_stride * 16 < (1L << 40) &&
+        planes < (1L << 31) && ((uintptr_t)in & 15) == 0 && ((uintptr_t)out & 15) == 0) {
+        switch (n + 1) {
+        case 64: return launch_wt<64>(c, ncols, planes, in, ld, plane_stride, out, lp);
+        case 128: return launch_wt<128>(c, ncols, planes, in, ld, plane_stride, out, lp);
+        case 256: return launch_wt<256>(c, ncols, planes, in, ld, plane_stride, out, lp);
+        case 512: return launch_wt<512>(c, ncols, planes, in, ld, plane_stride, out, lp);
+        default: break;
+        }
+    }
     // tensor maps need 16-byte aligned bases (always true for double2) and byte strides below 2^40
     // (the tensor-map box never exceeds the tensor: at least LPW columns)
     if (planes > 0 && ld * 16 < (1L << 40) && plane_stride * 16 < (1L << 40) && planes < (1L << 31)) {

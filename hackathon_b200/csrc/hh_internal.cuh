@@ -73,6 +73,7 @@ struct Ctx {
     std::vector<Plan *>      plans;
     long long                launches = 0;       // kernels launched through this context
     int                     *err_word = nullptr; // set by kernels whose bounded waits expire
+    size_t                   l2_bytes = 0;        // the device's L2 size (3D transform slabs)
     // stage timing (hh_ctx_set_stage_timing)
     bool                     timing = false;
     std::vector<cudaEvent_t> ev_pending;          // groups of 4 events per timed solve
@@ -111,6 +112,8 @@ struct Plan {
     double2 *Pv = nullptr;
     bool     const_rows = false; // stencil row tables constant along the line
     int      variant = 0;        // line-solve kernel: 0/1 general (512x1, 256x2), 2..6 symmetric
+    long     slab = 0;           // 3D: planes per slab of the transform passes (0: the whole batch)
+    int      col_kernel = 0;     // 3D column DST: 0 CTA tiles of 8 swizzled columns, 1 per-warp tiles
     bool     sym = false;        // const_rows and sub == super on every line (constant k)
     bool     pf_ok = false;      // order-6 partial fractions well conditioned on every line
     double2 *subt = nullptr, *diagt = nullptr; // sub/diagonal row tables (4 * rows each)
@@ -129,8 +132,9 @@ struct Plan {
 // kernels serve (n + 1 = 64 .. 1024); FP64 otherwise
 int launch_dst_rows(Ctx *c, int n, long rows, const double2 *in, long in_ld, double2 *out, long out_ld,
                     bool lp = false);
+// kern: 0 = CTA tiles of 8 swizzled columns where the length allows, 1 = per-warp tiles of LPW columns
 int launch_dst_cols(Ctx *c, int n, long ncols, long planes, const double2 *in, long ld, long plane_stride,
-                    double2 *out, bool lp = false);
+                    double2 *out, bool lp = false, int kern = 0);
 int launch_factor(Plan *p, const double2 *subt, const double2 *diagt, const double2 *supt);
 int launch_line_solve(Plan *p, const double2 *in, double2 *out, int batch, int src_order);
 // res = A_h u - rhs (FP64, zero Dirichlet ring); norms (optional, zeroed by the caller) receive
@@ -139,6 +143,7 @@ int launch_residual(Plan *p, const double2 *u, const double2 *rhs, double2 *res,
                     unsigned long long *norms);
 int launch_axpy(Ctx *c, double2 *u, const double2 *v, double s, long n); // u += s v
 int read_device_error(Ctx *c, int *val);
+long slab_planes(const Plan &p, long planes); // 3D transform slab in planes (the plan's or the default)
 int segment_count(int rows);
 int sym_default_variant(int rows);
 int padded_rows(int rows);

@@ -95,10 +95,28 @@ __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bu
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// A tiled tensor map of complex doubles seen as FLOAT64 pairs: dims[0] = 2 (re, im), strides in
-// bytes for dims[1..rank-1] (multiples of 16), box extents per dimension (<= 256).
+// 3-D tensor copies over (double, row, plane) maps: one box at double offset x (a multiple of 2,
+// so that x * 8 bytes stays on a 16-byte boundary), row j, plane p
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int j, int p, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            smem_u32(dst)),
+        "l"(map), "r"(x), "r"(j), "r"(p), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, int x, int j, int p, const void *src) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map),
+                 "r"(x), "r"(j), "r"(p), "r"(smem_u32(src))
+                 : "memory");
+}
+
+// A tiled tensor map of FLOAT64 values: dims[0] innermost (for complex data 2 = (re, im), or the
+// doubles of a whole row), strides in bytes for dims[1..rank-1] (multiples of 16), box extents
+// per dimension (<= 256).  swizzle128: 128-byte swizzle (box dims[0] * 8 must be 128 bytes; the
+// 16-byte chunk c of the box's 128-byte row r lands at chunk c ^ (r % 8) of a 1024-byte aligned
+// destination).
 int encode_tensor_map(CUtensorMap *map, const void *base, int rank, const unsigned long long *dims,
-                      const unsigned long long *strides, const unsigned *box);
+                      const unsigned long long *strides, const unsigned *box, bool swizzle128 = false);
 
 } // namespace hh
 

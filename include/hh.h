@@ -117,6 +117,20 @@ int hh_plan_tune(hh_plan *plan, int batch);
 int hh_plan_set_variant(hh_plan *plan, int variant);
 int hh_plan_variant(const hh_plan *plan);
 
+/* 3D plans: the transform passes can run slab by slab (rows pass over a slab of planes, then the
+ * columns pass over the same slab while the rows pass's output is still in L2).  `planes` per
+ * slab; 0 (the default) makes the whole batch one slab.  hh_plan_tune also times a few slab
+ * sizes for 3D plans and keeps the fastest.  The result does not depend on the slab. */
+int  hh_plan_set_slab(hh_plan *plan, long planes);
+long hh_plan_slab(const hh_plan *plan);
+/* 3D plans: the kernel of the transform along y (columns): 0 (the default) brings 8 neighbouring
+ * columns of all rows into a CTA as 128-byte-wide swizzled tensor boxes, 1 gives each warp its own
+ * tiles of as many columns as it transforms at once (2 at n = 255).  Lengths n + 1 = 64 .. 512 have
+ * both; other lengths use the second.  hh_plan_tune times both for 3D plans.  The result does
+ * not depend on the variant. */
+int  hh_plan_set_dst_variant(hh_plan *plan, int variant);
+int  hh_plan_dst_variant(const hh_plan *plan);
+
 /* Solve A u = rhs for `batch` assembled right-hand sides (the reference's solver(System),
  * 2D_Program/solver_functions/solver.c:14, 3D_Program/solver_functions/solver.c:263). */
 int hh_solve(hh_plan *plan, const double *rhs_dev, double *sol_dev, int batch);

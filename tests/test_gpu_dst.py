@@ -83,8 +83,12 @@ def test_dst_rows_pitched(ctx, oracle, n):
 
 
 @pytest.mark.parametrize("n,ncols,planes", [(255, 255, 3), (63, 100, 2), (100, 37, 2), (1023, 64, 1), (7, 5, 4),
-                                              (127, 33, 3), (511, 7, 2), (255, 1, 5), (63, 3, 7)])
+                                              (127, 33, 3), (511, 7, 2), (255, 1, 5), (63, 3, 7), (255, 8, 3),
+                                              (255, 16, 2), (511, 24, 2), (127, 9, 4), (63, 255, 1)])
 def test_dst_cols_matches_oracle(ctx, oracle, n, ncols, planes):
+    """Columns of planes: n + 1 = 64 .. 512 with at least 8 columns take the CTA-tile kernel
+    (8 swizzled columns per tensor box; counts that leave the last tile partly outside the plane),
+    narrower planes and other lengths the per-warp tiles or the first-design kernels."""
     rng = np.random.default_rng(n + ncols)
     x = rng.standard_normal((planes, n, ncols)) + 1j * rng.standard_normal((planes, n, ncols))
     t = _dev(x)

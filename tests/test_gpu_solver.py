@@ -2,7 +2,7 @@
 bit-exact with the reference's C code (tests/test_oracle.py)."""
 import numpy as np
 import pytest
-from conftest import assert_parity_2d, golden, rel_err
+from conftest import FACTOR_ASSEMBLED, assert_parity_2d, golden, rel_err
 
 import hackathon_b200 as hh
 from hackathon_b200 import workload as W
@@ -25,7 +25,7 @@ def test_solver2d_assembled_rhs_matches_oracle(ctx, oracle, n, order, k):
     ref = oracle.pipeline_2d(n, order, k, f)
     plan = hh.Plan.from_coefficients_2d(ctx, n, n, ref["coef"])
     sol = plan.solve_host(ref["rhs"])
-    assert_parity_2d(oracle, sol, ref, TOL)
+    assert_parity_2d(oracle, sol, ref, TOL, FACTOR_ASSEMBLED)
     plan.close()
 
 
@@ -222,3 +222,47 @@ def test_invalid_arguments(ctx):
     with pytest.raises(hh.HHError):
         plan.solve(0, 0, 1)
     plan.solve(0, 0, 0)  # empty batch is a no-op
+
+
+def test_3d_transform_slabs_give_identical_results(ctx, oracle):
+    """The 3D transforms run slab by slab (rows pass then columns pass per slab of planes); the
+    slab changes only the order of the launches, never a value: every slab size gives the same
+    bits, and they match the oracle."""
+    n, order, k, B = 63, 6, 30.0, 3
+    f_ext = [W.source_3d(n, W.sine_modes(40 + b, 16, 32, dim=3)) for b in range(B)]
+    f = np.stack([x[1:-1, 1:-1, 1:-1] for x in f_ext])
+    plan = hh.Plan.helmholtz(ctx, 3, n, order, k)
+    outs = []
+    for slab in (0, 1, 5, 63, 64, 189):
+        plan.slab = slab
+        assert plan.slab == slab
+        outs.append(plan.solve_source_host(f))
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])
+    assert rel_err(outs[0][1], oracle.pipeline_3d(n, order, k, f_ext[1])["sol"]) < TOL
+    plan.tune(B)
+    assert 1 <= plan.slab <= n * B
+    assert np.array_equal(plan.solve_source_host(f), outs[0])
+    with pytest.raises(hh.HHError):
+        plan.slab = -1
+    plan.close()
+
+
+@pytest.mark.parametrize("n", [63, 127, 255])
+def test_3d_column_dst_variants_give_identical_results(ctx, oracle, n):
+    """The two column-transform kernels of the 3D plans (CTA tiles of 8 swizzled columns, or
+    per-warp tiles) run the same transform arithmetic on the same values: identical bits."""
+    order, k, B = 6, 20.0, 2
+    f_ext = [W.source_3d(n, W.sine_modes(70 + b, 16, min(n, 64), dim=3)) for b in range(B)]
+    f = np.stack([x[1:-1, 1:-1, 1:-1] for x in f_ext])
+    plan = hh.Plan.helmholtz(ctx, 3, n, order, k)
+    outs = []
+    for v in (0, 1):
+        plan.dst_variant = v
+        assert plan.dst_variant == v
+        outs.append(plan.solve_source_host(f))
+    assert np.array_equal(outs[0], outs[1])
+    assert rel_err(outs[0][0], oracle.pipeline_3d(n, order, k, f_ext[0])["sol"]) < TOL
+    with pytest.raises(hh.HHError):
+        plan.dst_variant = 2
+    plan.close()
