@@ -63,6 +63,11 @@ SIGNATURES = {
     "hh_plan_tune": (_i, [_vp, _i]),
     "hh_plan_set_variant": (_i, [_vp, _i]),
     "hh_plan_variant": (_i, [_vp]),
+    "hh_plan_apply_tuning": (_i, [_vp, C.POINTER(_i)]),
+    "hh_tune_cache_stats": (_i, [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "hh_tune_cache_clear": (_i, []),
+    "hh_tune_cache_save": (_i, [C.c_char_p]),
+    "hh_tune_cache_load": (_i, [C.c_char_p, C.POINTER(C.c_longlong)]),
     "hh_plan_set_slab": (_i, [_vp, _l]),
     "hh_plan_slab": (_l, [_vp]),
     "hh_plan_set_dst_variant": (_i, [_vp, _i]),
@@ -232,9 +237,16 @@ class Plan:
             pass
 
     def tune(self, batch: int) -> int:
-        """Time the line-solve variants on `batch` right-hand sides, keep the fastest."""
+        """Time the line-solve variants on `batch` right-hand sides, keep the fastest (or apply the
+        tuning cache's entry for this shape)."""
         check(lib().hh_plan_tune(self.h, batch), "hh_plan_tune")
         return self.variant
+
+    def apply_tuning(self) -> bool:
+        """Apply the tuning cache's entry for this plan's shape, if any (never measures)."""
+        found = C.c_int()
+        check(lib().hh_plan_apply_tuning(self.h, C.byref(found)), "hh_plan_apply_tuning")
+        return bool(found.value)
 
     @property
     def variant(self) -> int:
@@ -315,6 +327,26 @@ class Plan:
         out = np.empty_like(f)
         check(lib().hh_solve_source_host(self.h, f.ctypes.data, out.ctypes.data, batch), "hh_solve_source_host")
         return out
+
+
+def tune_cache_stats() -> dict:
+    h, m, e = C.c_longlong(), C.c_longlong(), C.c_longlong()
+    check(lib().hh_tune_cache_stats(C.byref(h), C.byref(m), C.byref(e)), "hh_tune_cache_stats")
+    return {"hits": h.value, "misses": m.value, "entries": e.value}
+
+
+def tune_cache_clear():
+    check(lib().hh_tune_cache_clear(), "hh_tune_cache_clear")
+
+
+def tune_cache_save(path: str):
+    check(lib().hh_tune_cache_save(os.fsencode(path)), "hh_tune_cache_save")
+
+
+def tune_cache_load(path: str) -> int:
+    n = C.c_longlong()
+    check(lib().hh_tune_cache_load(os.fsencode(path), C.byref(n)), "hh_tune_cache_load")
+    return n.value
 
 
 def coefficients(dim: int, n: int, order: int, k: complex) -> dict:

@@ -555,9 +555,7 @@ static int transform_inverse(Plan &p, double2 *buf, int batch, bool lp = false);
 
 // Times every line-solve variant on `batch` zero right-hand sides (the solve does the same work
 // for any values) and keeps the fastest.  Blocks; must not run inside a stream capture.
-extern "C" int hh_plan_tune(hh_plan *pl, int batch) {
-    HH_TRY(check_batch(pl, batch));
-    if (batch == 0) return HH_OK;
+static int tune_measure(hh_plan *pl, int batch) {
     Plan &p = pl->p;
     Ctx  *c = p.ctx;
     HH_CUDA(cudaSetDevice(c->device));
@@ -638,6 +636,137 @@ extern "C" int hh_plan_tune(hh_plan *pl, int batch) {
     }
     if (rc == HH_OK) rc = hh_ctx_synchronize(reinterpret_cast<hh_ctx *>(c)); // Ctx is hh_ctx's first member
     return rc;
+}
+
+// ------------------------------------------------------------------ tuning cache ------
+// The kernel settings hh_plan_tune measures (line-solve variant; for 3D plans also the column
+// transform kernel and the transform slab), remembered per device model and problem shape: dim,
+// sizes, the fused source order and which line-solve kernels the plan's stencil admits.  The
+// wavenumber does not change which kernel is fastest (every variant does the same work for any
+// coefficients), so plans of one shape at different k share an entry.  Process-wide, guarded by a
+// mutex; hh_tune_cache_save / _load keep it in a text file (one tab-separated entry per line).
+namespace {
+struct TuneEntry {
+    int  variant = 0, col_kernel = 0;
+    long slab = 0;
+};
+std::mutex                       g_tune_mu;
+std::map<std::string, TuneEntry> g_tune;
+long long                        g_tune_hits = 0, g_tune_misses = 0;
+
+std::string tune_key(const Plan &p) {
+    char                   buf[512];
+    cudaDeviceProp         prop;
+    const char            *name = cudaGetDeviceProperties(&prop, p.ctx->device) == cudaSuccess ? prop.name : "unknown";
+    const int              kinds = p.sym ? (p.pf_ok ? 2 : 1) : 0;
+    snprintf(buf, sizeof buf, "%s\t%d\t%d\t%d\t%d\t%d\t%d", name, p.dim, p.nx, p.ny, p.nz, p.src_order, kinds);
+    return buf;
+}
+
+bool tune_apply(Plan &p, const TuneEntry &e) {
+    if (e.variant < 0 || e.variant >= solve_variant_count() || (e.variant >= 2 && !p.sym) || e.col_kernel < 0 ||
+        e.col_kernel > 1 || e.slab < 0)
+        return false;
+    p.variant = e.variant;
+    p.col_kernel = e.col_kernel;
+    p.slab = e.slab;
+    return true;
+}
+} // namespace
+
+// Applies the cached settings of the plan's shape; *found = 0 (plan unchanged) when there are none.
+extern "C" int hh_plan_apply_tuning(hh_plan *pl, int *found) {
+    if (!pl || !found) { set_error("hh_plan_apply_tuning: invalid arguments"); return HH_ERR_INVALID; }
+    const std::string key = tune_key(pl->p);
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    auto it = g_tune.find(key);
+    *found = it != g_tune.end() && tune_apply(pl->p, it->second);
+    return HH_OK;
+}
+
+extern "C" int hh_plan_tune(hh_plan *pl, int batch) {
+    HH_TRY(check_batch(pl, batch));
+    if (batch == 0) return HH_OK;
+    int found = 0;
+    HH_TRY(hh_plan_apply_tuning(pl, &found));
+    if (found) {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        g_tune_hits++;
+        return HH_OK;
+    }
+    HH_TRY(tune_measure(pl, batch));
+    TuneEntry e;
+    e.variant = pl->p.variant;
+    e.col_kernel = pl->p.col_kernel;
+    e.slab = pl->p.slab;
+    const std::string key = tune_key(pl->p);
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tune[key] = e;
+    g_tune_misses++;
+    return HH_OK;
+}
+
+extern "C" int hh_tune_cache_stats(long long *hits, long long *misses, long long *entries) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    if (hits) *hits = g_tune_hits;
+    if (misses) *misses = g_tune_misses;
+    if (entries) *entries = (long long)g_tune.size();
+    return HH_OK;
+}
+
+extern "C" int hh_tune_cache_clear(void) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tune.clear();
+    g_tune_hits = g_tune_misses = 0;
+    return HH_OK;
+}
+
+extern "C" int hh_tune_cache_save(const char *path) {
+    if (!path) { set_error("hh_tune_cache_save: null path"); return HH_ERR_INVALID; }
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    FILE *f = fopen(path, "w");
+    if (!f) { set_error("hh_tune_cache_save: cannot write %s", path); return HH_ERR_INVALID; }
+    fprintf(f, "# hackathon_b200 tuning cache: device, dim, nx, ny, nz, source order, kernels, variant, column kernel, slab\n");
+    for (auto &kv : g_tune) fprintf(f, "%s\t%d\t%d\t%ld\n", kv.first.c_str(), kv.second.variant, kv.second.col_kernel, kv.second.slab);
+    const bool ok = fclose(f) == 0;
+    if (!ok) { set_error("hh_tune_cache_save: write error on %s", path); return HH_ERR_INVALID; }
+    return HH_OK;
+}
+
+// Adds the entries of a file written by hh_tune_cache_save (malformed lines are skipped);
+// *loaded (optional) receives the number of entries read.
+extern "C" int hh_tune_cache_load(const char *path, long long *loaded) {
+    if (!path) { set_error("hh_tune_cache_load: null path"); return HH_ERR_INVALID; }
+    FILE *f = fopen(path, "r");
+    if (!f) { set_error("hh_tune_cache_load: cannot read %s", path); return HH_ERR_INVALID; }
+    char      line[1024];
+    long long n = 0;
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    while (fgets(line, sizeof line, f)) {
+        if (line[0] == '#') continue;
+        // the last three tab-separated fields are the settings, the rest is the key
+        std::string l(line);
+        while (!l.empty() && (l.back() == '\n' || l.back() == '\r')) l.pop_back();
+        size_t cut[3];
+        size_t pos = l.size();
+        bool   ok = true;
+        for (int t = 0; t < 3 && ok; t++) {
+            pos = l.rfind('\t', pos == 0 ? 0 : pos - 1);
+            ok = pos != std::string::npos && pos > 0;
+            cut[t] = pos;
+        }
+        if (!ok) continue;
+        TuneEntry e;
+        char     *end = nullptr;
+        e.variant = (int)strtol(l.c_str() + cut[2] + 1, &end, 10);
+        e.col_kernel = (int)strtol(l.c_str() + cut[1] + 1, &end, 10);
+        e.slab = strtol(l.c_str() + cut[0] + 1, &end, 10);
+        g_tune[l.substr(0, cut[2])] = e;
+        n++;
+    }
+    fclose(f);
+    if (loaded) *loaded = n;
+    return HH_OK;
 }
 
 // -------------------------------------------------------------------- solve ------

@@ -117,6 +117,19 @@ int hh_plan_tune(hh_plan *plan, int batch);
 int hh_plan_set_variant(hh_plan *plan, int variant);
 int hh_plan_variant(const hh_plan *plan);
 
+/* Tuning cache (the reference launches fixed shapes: grid = (numSMs, numSMs), block = (16, 16),
+ * 3D_Program/solver_functions/cuda_kernels.cu:336-346).  hh_plan_tune remembers what it measured
+ * per device model and problem shape (dim, nx, ny, nz, fused source order, and which line-solve
+ * kernels the stencil admits; not k, which does not change which kernel is fastest) and applies
+ * a remembered entry instead of timing: a cache hit launches nothing.  The cache is process-wide
+ * and thread-safe.  hh_plan_apply_tuning applies an entry if one exists (*found = 1) and never
+ * measures.  save/load keep the cache in a text file; load adds to what is cached. */
+int hh_plan_apply_tuning(hh_plan *plan, int *found);
+int hh_tune_cache_stats(long long *hits, long long *misses, long long *entries);
+int hh_tune_cache_clear(void);
+int hh_tune_cache_save(const char *path);
+int hh_tune_cache_load(const char *path, long long *loaded);
+
 /* 3D plans: the transform passes can run slab by slab (rows pass over a slab of planes, then the
  * columns pass over the same slab while the rows pass's output is still in L2).  `planes` per
  * slab; 0 (the default) makes the whole batch one slab.  hh_plan_tune also times a few slab
