@@ -388,22 +388,57 @@ SERVE_2D = [63, 127, 255, 511, 1023, 2047]
 SERVE_3D = [31, 63, 127, 255]
 
 
+def device_sources(torch, dim: int, n: int, count: int, seed0: int):
+    """`count` seeded sine-mode sources at the interior points, built on the device: in 2D 8 modes
+    with p, q <= min(20, n) (the generator of the 2D configurations without noise), in 3D 16 modes
+    with p, q, r <= min(64, n); seeds seed0 + b.  Complex amplitudes CN(0, 1)."""
+    from hackathon_b200 import workload as W
+    nm, pmax = (8, min(20, n)) if dim == 2 else (16, min(64, n))
+    x = torch.arange(1, n + 1, dtype=torch.float64, device="cuda") / (n + 1)
+    out = torch.empty((count,) + (n,) * dim, dtype=torch.complex128, device="cuda")
+    for b in range(count):
+        m = W.sine_modes(seed0 + b, nm, pmax, dim=dim)
+        amp = torch.from_numpy(m.amp).cuda()
+        sp = torch.sin(math.pi * torch.from_numpy(m.p).cuda().double()[:, None] * x[None, :]).to(torch.complex128)
+        sq = torch.sin(math.pi * torch.from_numpy(m.q).cuda().double()[:, None] * x[None, :]).to(torch.complex128)
+        if dim == 2:
+            out[b] = torch.einsum("m,my,mx->yx", amp, sq, sp)
+        else:
+            sr = torch.sin(math.pi * torch.from_numpy(m.r).cuda().double()[:, None] * x[None, :]).to(torch.complex128)
+            out[b] = torch.einsum("m,mz,my,mx->zyx", amp, sr, sq, sp)
+    return out
+
+
+def serve_pretune(hh, batch: int = 8) -> float:
+    """Tune one plan per served shape (dim, n, order) before serving: the request loop's new plans
+    take these settings from the tuning cache.  Returns the seconds spent (not served time)."""
+    t0 = time.perf_counter()
+    ctx = hh.Context(0)
+    for dim, sizes in ((2, SERVE_2D), (3, SERVE_3D)):
+        for n in sizes:
+            for order in (2, 4, 6):
+                p = hh.Plan.helmholtz(ctx, dim, n, order, 100.0)
+                p.tune(batch)
+                p.close()
+    ctx.close()
+    return time.perf_counter() - t0
+
+
 def serve_run(hh, torch, seconds: float = 2.0, rate: float = 2000.0, seed: int = 5, budget: int = 150 << 30,
-              streams: int = 4) -> dict:
+              streams: int = 4, bufs=None) -> dict:
     """The serving configuration: Poisson arrivals (mean `rate` per second) for `seconds`, sizes
     drawn uniformly from 2D N in {63..2047} and 3D N in {31..255} (log-uniform in N), order in
     {2, 4, 6}, k ~ U[1, 200], 1..32 right-hand sides, through the native request loop with an HBM
-    budget.  Inputs are seeded normal samples resident on the device (one 32-RHS buffer per
+    budget.  Inputs are seeded sine-mode sources resident on the device (one 32-RHS buffer per
     size, shared by the requests of that size); latency is submit -> completion on the server's
     clock."""
     rng = np.random.default_rng(seed)
     sizes = [(2, n) for n in SERVE_2D] + [(3, n) for n in SERVE_3D]
-    gen = torch.Generator(device="cuda").manual_seed(seed)
-    bufs = {}
-    for dim, n in sizes:
-        shape = (32,) + (n,) * dim
-        f = torch.randn(shape, dtype=torch.complex128, device="cuda", generator=gen)
-        bufs[(dim, n)] = (f, torch.empty_like(f))
+    if bufs is None:
+        bufs = {}
+        for i, (dim, n) in enumerate(sizes):
+            f = device_sources(torch, dim, n, 32, 4000 + 100 * i)
+            bufs[(dim, n)] = (f, torch.empty_like(f))
     torch.cuda.synchronize()
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=int(rate * seconds * 1.5) + 16))
     arrivals = arrivals[arrivals < seconds]
@@ -426,12 +461,33 @@ def serve_run(hh, torch, seconds: float = 2.0, rate: float = 2000.0, seed: int =
     rhs = sum(r[4] for r in reqs)
     t_end = max(x["t_done"] for x in infos) - t0
     pts = sum(r[4] * r[1] ** r[0] for r in reqs)
+    offered_pts = pts / seconds
+    peak = measured_hbm_peak()[0]
     return {"requests": len(reqs), "right_hand_sides": rhs, "offered_rate_per_s": rate, "arrival_window_s": seconds,
             "makespan_s": t_end, "requests_per_s": len(reqs) / t_end, "solves_per_s": rhs / t_end,
             "gpoints_per_s": pts / t_end / 1e9, "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "mean_batch_rhs": float(np.mean([x["batch_rhs"] for x in infos])),
             "plans_resident_at_end": stats["plans"], "hbm_budget_gb": budget / 2 ** 30, "streams": streams,
-            "inputs": "device-resident seeded normal samples; form plain FP64"}
+            "offered_gpoints_per_s": offered_pts / 1e9,
+            "offered_hbm_gbs_at_96B_per_point": 96.0 * offered_pts / 1e9,
+            "offered_vs_hbm_roofline": 96.0 * offered_pts / 1e9 / peak,
+            "inputs": "device-resident seeded sine-mode sources; form plain FP64; plans tuned per shape beforehand"}
+
+
+def serving_block(hh, torch, seconds: float = 1.0, rate: float = 2000.0) -> dict:
+    """The configured stream, then the same mix at 80 % of the request rate the device completed
+    on it (latency under a load it sustains)."""
+    sizes = [(2, n) for n in SERVE_2D] + [(3, n) for n in SERVE_3D]
+    bufs = {}
+    for i, (dim, n) in enumerate(sizes):
+        f = device_sources(torch, dim, n, 32, 4000 + 100 * i)
+        bufs[(dim, n)] = (f, torch.empty_like(f))
+    pre = serve_pretune(hh)
+    res = serve_run(hh, torch, seconds=seconds, rate=rate, bufs=bufs)
+    sus = serve_run(hh, torch, seconds=seconds, rate=0.8 * res["requests_per_s"], seed=6, bufs=bufs)
+    del bufs
+    torch.cuda.empty_cache()
+    return {"configured": res, "sustainable": sus, "pretune_s": pre}
 
 
 def main():
@@ -466,14 +522,10 @@ def main():
     if args.serve:
         if rank == 0:
             torch.cuda.set_device(local)
-            res = serve_run(hh, torch, seconds=args.serve_seconds, rate=args.serve_rate)
-            # the configured stream offers more work than the device completes; latency under a load
-            # it sustains: the same mix at the rate the device just completed requests, times 0.8
-            sustained = serve_run(hh, torch, seconds=args.serve_seconds, rate=0.8 * res["requests_per_s"], seed=6)
+            blk = serving_block(hh, torch, seconds=args.serve_seconds, rate=args.serve_rate)
             print(json.dumps({"metric": "serving p50/p99 latency and solves/s under the mixed 2D/3D request stream",
-                              "value": res["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
-                              "higher_is_better": True, "impl": "ours", "mode": "serve", "serving": res,
-                              "serving_at_sustainable_rate": sustained}), flush=True)
+                              "value": blk["configured"]["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+                              "higher_is_better": True, "impl": "ours", "mode": "serve", "serving": blk}), flush=True)
         return
 
     batch = args.batch
@@ -619,7 +671,7 @@ def main():
         if world == 1 and not args.no_secondary:
             line["secondary"] = secondary_configs(hh, ctx, st, torch)
             line["secondary"]["mixed_precision_refined"] = refined_configs(hh, ctx, st, torch)
-            line["secondary"]["serving"] = serve_run(hh, torch, seconds=1.0)
+            line["secondary"]["serving"] = serving_block(hh, torch, seconds=1.0)
         def gpu_solve(order, k, f_int):
             return plans[COMBOS.index((order, k))].solve_source_host(f_int)
 

@@ -47,6 +47,7 @@ SIGNATURES = {
     "hh_ctx_set_stream": (_i, [_vp, _vp]),
     "hh_ctx_synchronize": (_i, [_vp]),
     "hh_ctx_launch_count": (C.c_longlong, [_vp]),
+    "hh_ctx_inject_wait_expiry": (_i, [_vp]),
     "hh_malloc": (_i, [_vp, _sz, C.POINTER(_vp)]),
     "hh_free": (_i, [_vp, _vp]),
     "hh_memcpy_h2d": (_i, [_vp, _vp, _vp, _sz]),
@@ -90,6 +91,7 @@ SIGNATURES = {
     "hh_server_clock": (_d, [_vp]),
     "hh_server_destroy": (_i, [_vp]),
     "hh_server_inject_error": (_i, [_vp, _i]),
+    "hh_server_inject_wait_expiry": (_i, [_vp]),
 }
 
 _lib = None
@@ -161,6 +163,10 @@ class Context:
 
     def synchronize(self):
         check(lib().hh_ctx_synchronize(self.h), "hh_ctx_synchronize")
+
+    def inject_wait_expiry(self):
+        """Arm one expired bounded wait in the next rows-transform launch (hh_ctx_inject_wait_expiry)."""
+        check(lib().hh_ctx_inject_wait_expiry(self.h), "hh_ctx_inject_wait_expiry")
 
     def set_stage_timing(self, on: bool):
         check(lib().hh_ctx_set_stage_timing(self.h, 1 if on else 0), "hh_ctx_set_stage_timing")
@@ -394,6 +400,10 @@ class Server:
 
     def clock(self) -> float:
         return float(lib().hh_server_clock(self.h))
+
+    def inject_wait_expiry(self):
+        """Arm one expired bounded wait on the loop's device (hh_server_inject_wait_expiry)."""
+        check(lib().hh_server_inject_wait_expiry(self.h), "hh_server_inject_wait_expiry")
 
     def inject_error(self, batches: int = 1):
         """The next `batches` batches complete with HH_ERR_DEVICE (hh_server_inject_error)."""

@@ -108,8 +108,9 @@ extern "C" int hh_ctx_create(int device, void *stream, hh_ctx **out) {
         if (e != cudaSuccess) { delete x; return cuda_fail(e, "cudaStreamCreateWithFlags", __FILE__, __LINE__); }
         x->c.own_stream = true;
     }
-    cudaError_t e = cudaMalloc(&x->c.err_word, sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(x->c.err_word, 0, sizeof(int));
+    cudaError_t e = cudaMalloc(&x->c.err_word, 2 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(x->c.err_word, 0, 2 * sizeof(int));
+    if (e == cudaSuccess) x->c.inject_word = x->c.err_word + 1;
     if (e == cudaSuccess) e = cudaGetSymbolAddress((void **)&x->noalloc_stage, g_noalloc_stage);
     if (e != cudaSuccess) {
         if (x->c.own_stream) cudaStreamDestroy(x->c.stream);
@@ -171,6 +172,15 @@ extern "C" int hh_ctx_synchronize(hh_ctx *x) {
 }
 
 extern "C" long long hh_ctx_launch_count(const hh_ctx *x) { return x ? x->c.launches : 0; }
+
+extern "C" int hh_ctx_inject_wait_expiry(hh_ctx *x) {
+    if (!x) { set_error("hh_ctx_inject_wait_expiry: null context"); return HH_ERR_INVALID; }
+    HH_CUDA(cudaSetDevice(x->c.device));
+    const int one = 1;
+    HH_CUDA(cudaMemcpyAsync(x->c.inject_word, &one, sizeof(int), cudaMemcpyHostToDevice, x->c.stream));
+    HH_CUDA(cudaStreamSynchronize(x->c.stream));
+    return HH_OK;
+}
 
 static void drain_events(Ctx &c) {
     if (!c.ev_pending.empty()) cudaEventSynchronize(c.ev_pending.back()); // all recorded events complete

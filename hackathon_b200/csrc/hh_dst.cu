@@ -728,10 +728,18 @@ __device__ __forceinline__ void w_transform_lp(XLoad xload, double2 *buf, int l,
 
 // ---- rows: lines g = 0 .. nlines*nplanes-1 at in + (g / nlines) in_plane + (g % nlines) in_ld
 // with x_1..x_N at offsets 0..N-1, likewise for the output; in and out may be the same buffer.
+// Failure injection (hh_ctx_inject_wait_expiry): when *inj is set, warp 0 of CTA 0 takes it
+// (one launch only) and its first line group's barrier expects kInjectBytes more than the copies
+// bring, so that wait cannot complete and runs out of a short poll budget (kInjectPolls); the
+// kernel then reports through `err` exactly as for a copy that never lands.  The drain counts
+// the added bytes as arrived itself and waits, with the full budget, for the real copies.
+constexpr uint32_t kInjectBytes = 16;
+constexpr long     kInjectPolls = 1L << 12;
+
 template <int M, bool LP = false>
 __global__ void __launch_bounds__(32 * WCfg<M>::WPC, WCfg<M>::MINB)
     k_dst1_w(const double2 *in, double2 *out, long nlines, long nplanes, long in_ld, long out_ld, long in_plane,
-             long out_plane, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
+             long out_plane, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err, int *inj) {
     using G = WGeom<M>;
     constexpr int      TL = G::TL, LPW = G::LPW, KB = G::KB, BUF = G::BUF, N = M - 1, K2 = 2 * KB;
     constexpr uint32_t kLineBytes = N * 16;
@@ -753,11 +761,14 @@ __global__ void __launch_bounds__(32 * WCfg<M>::WPC, WCfg<M>::MINB)
     auto dst_of = [&](long g) {
         return nplanes == 1 ? out + g * out_ld : out + (g / nlines) * out_plane + (g % nlines) * out_ld;
     };
-    // lane 0: bring in line group `grp` to buffer set `s`
-    auto fetch = [&](long grp, int s) {
+    int injected = 0;
+    if (lane == 0 && inj && blockIdx.x == 0 && wq == 0) injected = atomicExch(inj, 0);
+    injected = __shfl_sync(0xffffffffu, injected, 0);
+    // lane 0: bring in line group `grp` to buffer set `s` (`extra`: injected bytes that never come)
+    auto fetch = [&](long grp, int s, uint32_t extra) {
         const long first = grp * LPW;
         const int  nl = (int)((total - first) < LPW ? (total - first) : LPW);
-        mbar_expect_tx(&bar[s], (uint32_t)nl * kLineBytes);
+        mbar_expect_tx(&bar[s], (uint32_t)nl * kLineBytes + extra);
         for (int x = 0; x < nl; x++) tma_bulk_load(sets + (s * LPW + x) * BUF, src_of(first + x), kLineBytes, &bar[s]);
     };
     if (lane == 0) {
@@ -768,8 +779,8 @@ __global__ void __launch_bounds__(32 * WCfg<M>::WPC, WCfg<M>::MINB)
     __syncwarp();
     constexpr int NBUF = G::NBUF;
     if (lane == 0) {
-        fetch(g0, 0);
-        if (NBUF == 2 && g0 + stride < groups) fetch(g0 + stride, 1);
+        fetch(g0, 0, injected ? kInjectBytes : 0u);
+        if (NBUF == 2 && g0 + stride < groups) fetch(g0 + stride, 1, 0u);
     }
     WConst<M> K;
     K.load(l, tw, sn);
@@ -781,7 +792,8 @@ __global__ void __launch_bounds__(32 * WCfg<M>::WPC, WCfg<M>::MINB)
         double2  *buf = sets + (s * LPW + c) * BUF;
         const long line = grp * LPW + c;
         const bool live = line < total;
-        if (!mbar_wait_parity(&bar[s], NBUF == 2 ? (it >> 1) & 1 : it & 1)) {
+        const uint32_t par = NBUF == 2 ? (it >> 1) & 1 : it & 1;
+        if (!(it == 0 && injected ? mbar_wait_parity_n(&bar[s], par, kInjectPolls) : mbar_wait_parity(&bar[s], par))) {
             if (lane == 0) atomicExch(err, 1);
             failed = grp;
             break;
@@ -800,10 +812,11 @@ __global__ void __launch_bounds__(32 * WCfg<M>::WPC, WCfg<M>::MINB)
         // generic-proxy accesses before the asynchronous copy that overwrites them)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncwarp();
-        if (lane == 0 && grp + NBUF * stride < groups) fetch(grp + NBUF * stride, s);
+        if (lane == 0 && grp + NBUF * stride < groups) fetch(grp + NBUF * stride, s, 0u);
     }
     // after an expired wait, give the copies still in flight a bounded chance to land before the
     // CTA's shared memory is released
+    if (failed >= 0 && lane == 0 && injected && it == 0) mbar_complete_tx(&bar[0], kInjectBytes);
     if (failed >= 0 && lane == 0) {
         if (NBUF == 1) {
             mbar_wait_parity(&bar[0], it & 1);
@@ -1308,7 +1321,8 @@ template <int M, bool LP> static int launch_wp(Ctx *c, const DstArgs &a) {
     const long groups = (a.nlines * a.planes + G::LPW - 1) / G::LPW;
     const long ctas = std::min<long>((groups + G::WPC - 1) / G::WPC, (long)std::max(1, per_sm) * sms);
     k_dst1_w<M, LP><<<(unsigned)ctas, 32 * G::WPC, G::SMEM, c->stream>>>(a.in, a.out, a.nlines, a.planes, a.in_ld, a.out_ld,
-                                                                     a.in_plane, a.out_plane, tw, sn, c->err_word);
+                                                                     a.in_plane, a.out_plane, tw, sn, c->err_word,
+                                                                     c->inject_word);
     HH_CUDA(cudaGetLastError());
     c->launches++;
     return HH_OK;

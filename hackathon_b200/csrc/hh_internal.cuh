@@ -73,6 +73,7 @@ struct Ctx {
     std::vector<Plan *>      plans;
     long long                launches = 0;       // kernels launched through this context
     int                     *err_word = nullptr; // set by kernels whose bounded waits expire
+    int                     *inject_word = nullptr; // armed by hh_ctx_inject_wait_expiry, taken by one launch
     size_t                   l2_bytes = 0;        // the device's L2 size (3D transform slabs)
     // stage timing (hh_ctx_set_stage_timing)
     bool                     timing = false;

@@ -4,7 +4,8 @@
 // loop keeps the solver's per-problem set-up resident and streams requests through it:
 //  * one plan per (dim, n, order, k) stays on the device (twiddles and sine tables are shared by
 //    the context, factors and Pade tables belong to the plan) and is evicted least recently used
-//    when the HBM budget needs the room;
+//    when the HBM budget needs the room; a new plan takes the kernel settings of its shape from
+//    the tuning cache (hh_plan_tune), if the process has tuned that shape;
 //  * continuous batching: when the dispatcher picks a request it also takes every queued request
 //    of the same plan (small ones, up to kMergeRhs right-hand sides in all) and runs them as one
 //    batched solve;
@@ -300,6 +301,8 @@ void dispatcher(hh_server *s) {
             if (rc == HH_OK)
                 rc = r.dim == 2 ? hh_plan2d_create_helmholtz(s->ctx, r.n, r.order, r.k_re, r.k_im, &plan)
                                 : hh_plan3d_create_helmholtz(s->ctx, r.n, r.order, r.k_re, r.k_im, &plan);
+            int tuned = 0; // the kernel settings hh_plan_tune found for this shape, if any (never measures)
+            if (rc == HH_OK) rc = hh_plan_apply_tuning(plan, &tuned);
             if (rc == HH_OK && cudaEventRecord(s->ready, s->setup) != cudaSuccess) rc = HH_ERR_CUDA;
             const std::string msg = rc == HH_OK ? std::string() : std::string(hh_last_error());
             fresh = rc == HH_OK;
@@ -464,6 +467,23 @@ extern "C" int hh_server_destroy(hh_server *s) {
     cudaFreeHost(s->flags);
     cudaFree(s->words);
     delete s;
+    return HH_OK;
+}
+
+extern "C" int hh_server_inject_wait_expiry(hh_server *s) {
+    if (!s) {
+        set_error("hh_server_inject_wait_expiry: null server");
+        return HH_ERR_INVALID;
+    }
+    // the dispatcher owns the context's stream: write the word synchronously instead
+    const int one = 1;
+    cudaError_t e = cudaSetDevice(s->device);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(reinterpret_cast<hh::Ctx *>(s->ctx)->inject_word, &one, sizeof(int), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        set_error("hh_server_inject_wait_expiry: %s", cudaGetErrorString(e));
+        return HH_ERR_CUDA;
+    }
     return HH_OK;
 }
 

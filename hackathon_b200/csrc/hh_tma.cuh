@@ -62,6 +62,26 @@ __device__ __forceinline__ bool mbar_wait_parity(uint64_t *bar, uint32_t parity)
     return false;
 }
 
+// the same wait with a caller-chosen poll budget (failure injection uses a short one)
+__device__ __forceinline__ bool mbar_wait_parity_n(uint64_t *bar, uint32_t parity, long polls) {
+    const uint32_t a = smem_u32(bar);
+    for (long it = 0; it < polls; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// counts `bytes` of the current phase's expected transaction bytes as arrived (the failure
+// injection's drain settles the bytes it added this way)
+__device__ __forceinline__ void mbar_complete_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.complete_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
 // Tensor copies (cp.async.bulk.tensor) need 128-byte aligned shared-memory addresses and a
 // tensor map whose innermost coordinate here is always 0 (the re/im pair of a complex double).
 __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, int c1, int c2, int c3, int c4,

@@ -788,7 +788,9 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
             const double2 *tl = tio.tin + (long)u * tio.tile + c;
 #pragma unroll
             for (int k = 0; k < KS; k++) v[0][k] = (r0 + k < rows) ? tl[(r0 + k) * CW] : zero;
-            gm[0] = (HALO && r0 > 0) ? tl[(r0 - 1) * CW] : zero;
+            // threads whose segment lies wholly past the end of the line (r0 > rows) read no halo:
+            // row r0 - 1 is not in the tile
+            gm[0] = (HALO && r0 > 0 && r0 <= rows) ? tl[(r0 - 1) * CW] : zero;
             gp[0] = (HALO && r0 + KS < rows) ? tl[(r0 + KS) * CW] : zero;
             fence_async_smem(); // these reads before the copy that refills the tile
         } else {

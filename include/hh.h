@@ -51,6 +51,13 @@ int hh_ctx_destroy(hh_ctx *ctx);
 int hh_ctx_set_stream(hh_ctx *ctx, void *stream);
 int hh_ctx_synchronize(hh_ctx *ctx);          /* also surfaces kernel-reported failures   */
 long long hh_ctx_launch_count(const hh_ctx *ctx); /* kernels launched through this context */
+/* Failure injection on the device (no counterpart in the reference): the next rows transform
+ * launched on the context with n + 1 in 64 .. 512 (the per-warp kernel of the 2D solves at those
+ * sizes and of the 3D x-transforms) makes one of its copies' barriers wait for 16 bytes that never
+ * arrive.  That bounded wait expires after a short budget, the kernel reports it, drains its own
+ * copies and ends; its output is incomplete and the next hh_ctx_synchronize returns
+ * HH_ERR_DEVICE (and clears it).  Nothing faults or hangs; the context stays usable. */
+int hh_ctx_inject_wait_expiry(hh_ctx *ctx);
 
 /* Stage timing: when enabled, every solve records CUDA events on the context's stream around
  * its three stages (forward transform, line solves, inverse transform) and accumulates the
@@ -196,7 +203,8 @@ int hh_coefficients3d(int n, int order, double k_re, double k_im, double *const 
  * one problem per process).  hh_server_submit queues a request and returns at once; a
  * dispatcher thread solves it asynchronously:
  *  - one plan per (dim, n, order, k) stays resident (least recently used plans are evicted
- *    when the HBM budget needs the room);
+ *    when the HBM budget needs the room); new plans take the tuning cache's settings for their
+ *    shape (hh_plan_apply_tuning), so tune one plan per served shape beforehand;
  *  - continuous batching: queued requests of the same plan (up to 64 right-hand sides, each
  *    request at most 4M points) run as one batched solve;
  *  - admission: a batch starts while plans plus in-flight staging fit the HBM budget, otherwise
@@ -231,6 +239,9 @@ int    hh_server_destroy(hh_server *s); /* finishes every submitted request firs
  * had reported an expired bounded wait.  Each stream has its own device error word, cleared
  * before every batch, so a failure is charged to its own batch only and later batches succeed. */
 int    hh_server_inject_error(hh_server *s, int batches);
+/* The device form: arms hh_ctx_inject_wait_expiry on the loop's context, so that the next batch
+ * that runs such a rows transform fails with HH_ERR_DEVICE through its own stream's error word. */
+int    hh_server_inject_wait_expiry(hh_server *s);
 
 #ifdef __cplusplus
 }
