@@ -78,6 +78,7 @@ SIGNATURES = {
     "hh_solve_source": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source_host": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source_host_noalloc": (_i, [_vp, _vp, _vp, _i]),
+    "hh_solve_source_multi": (_i, [C.POINTER(_vp), C.POINTER(_i), _i, _vp, _vp]),
     "hh_residual": (_i, [_vp, _vp, _vp, _vp, _i, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "hh_solve_refined": (_i, [_vp, _vp, _vp, _i, C.c_double, _i, C.POINTER(_i), C.POINTER(C.c_double)]),
     "hh_coefficients2d": (_i, [_i, _i, _d, _d, C.POINTER(_vp)]),
@@ -333,6 +334,14 @@ class Plan:
         out = np.empty_like(f)
         check(lib().hh_solve_source_host(self.h, f.ctypes.data, out.ctypes.data, batch), "hh_solve_source_host")
         return out
+
+
+def solve_source_multi(plans, nrhs, f, u):
+    """hh_solve_source_multi: plans of one shape, plan i taking nrhs[i] consecutive fields of the
+    device buffers f and u."""
+    hs = (_vp * len(plans))(*[p.h for p in plans])
+    ns = (_i * len(plans))(*nrhs)
+    check(lib().hh_solve_source_multi(hs, ns, len(plans), _addr(f), _addr(u)), "hh_solve_source_multi")
 
 
 def tune_cache_stats() -> dict:

@@ -98,9 +98,12 @@ extern "C" int hh_ctx_create(int device, void *stream, hh_ctx **out) {
     HH_CUDA(cudaSetDevice(device));
     int l2 = 0;
     HH_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device));
+    cudaDeviceProp prop;
+    HH_CUDA(cudaGetDeviceProperties(&prop, device)); // once per context: the query is slow
     hh_ctx *x = new hh_ctx();
     x->c.device = device;
     x->c.l2_bytes = l2 > 0 ? (size_t)l2 : (size_t)(50u << 20);
+    x->c.dev_name = prop.name;
     if (stream) {
         x->c.stream = (cudaStream_t)stream;
     } else {
@@ -141,6 +144,7 @@ extern "C" int hh_ctx_destroy(hh_ctx *x) {
     cudaFree(x->c.err_word);
     cudaFree(x->c.norms);
     cudaFree(x->c.refine_work);
+    cudaFree(x->c.multi_tab);
     cudaFree(x->stage);
     for (cudaEvent_t e : x->c.chunk_ev) cudaEventDestroy(e);
     if (x->c.copy_in) cudaStreamDestroy(x->c.copy_in);
@@ -665,11 +669,10 @@ std::map<std::string, TuneEntry> g_tune;
 long long                        g_tune_hits = 0, g_tune_misses = 0;
 
 std::string tune_key(const Plan &p) {
-    char                   buf[512];
-    cudaDeviceProp         prop;
-    const char            *name = cudaGetDeviceProperties(&prop, p.ctx->device) == cudaSuccess ? prop.name : "unknown";
-    const int              kinds = p.sym ? (p.pf_ok ? 2 : 1) : 0;
-    snprintf(buf, sizeof buf, "%s\t%d\t%d\t%d\t%d\t%d\t%d", name, p.dim, p.nx, p.ny, p.nz, p.src_order, kinds);
+    char      buf[512];
+    const int kinds = p.sym ? (p.pf_ok ? 2 : 1) : 0;
+    snprintf(buf, sizeof buf, "%s\t%d\t%d\t%d\t%d\t%d\t%d", p.ctx->dev_name.c_str(), p.dim, p.nx, p.ny, p.nz,
+             p.src_order, kinds);
     return buf;
 }
 
@@ -971,6 +974,72 @@ extern "C" int hh_solve_source(hh_plan *pl, const double *f, double *u, int batc
     HH_TRY(stage_mark(*p.ctx, 2));
     HH_TRY(transform_inverse(p, w, batch));
     return stage_mark(*p.ctx, 3);
+}
+
+// Several wavenumbers in one solve: plans of one shape (dim, sizes, fused order) on one context,
+// plan i taking nrhs[i] consecutive fields of f and u.  The transforms do not depend on k, so each
+// direction is one launch over the whole batch; the line solves are one launch with a table of
+// which right-hand sides use which plan's factors (or one launch per plan where the plans do not
+// share a symmetric kernel variant).  table: device memory for that table (nullptr: the context's
+// own, grown on demand, which orders the solve behind earlier work on the context's stream).
+int hh::solve_source_multi(Plan *const *plans, const int *nrhs, int nplans, const double2 *f, double2 *u,
+                           void *table) {
+    Plan &p0 = *plans[0];
+    Ctx  *c = p0.ctx;
+    int   total = 0;
+    for (int i = 0; i < nplans; i++) total += nrhs[i];
+    if (total == 0) return HH_OK;
+    HH_TRY(stage_mark(*c, 0));
+    HH_TRY(transform_forward(p0, f, u, total));
+    HH_TRY(stage_mark(*c, 1));
+    if (!table) {
+        const size_t need = line_solve_multi_table_bytes(nplans, total);
+        if (c->multi_tab_bytes < need) {
+            HH_CUDA(cudaStreamSynchronize(c->stream));
+            cudaFree(c->multi_tab);
+            c->multi_tab = nullptr;
+            c->multi_tab_bytes = 0;
+            HH_CUDA(cudaMalloc(&c->multi_tab, need));
+            c->multi_tab_bytes = need;
+        }
+        table = c->multi_tab;
+    }
+    int rc = nplans > 1 ? launch_line_solve_multi(plans, nrhs, nplans, u, u, p0.src_order, table) : HH_ERR_UNSUPPORTED;
+    if (rc == HH_ERR_UNSUPPORTED) { // one launch per plan
+        rc = HH_OK;
+        long off = 0;
+        for (int i = 0; i < nplans && rc == HH_OK; i++) {
+            if (nrhs[i]) rc = launch_line_solve(plans[i], u + off, u + off, nrhs[i], p0.src_order);
+            off += p0.field * nrhs[i];
+        }
+    }
+    HH_TRY(rc);
+    HH_TRY(stage_mark(*c, 2));
+    HH_TRY(transform_inverse(p0, u, total));
+    return stage_mark(*c, 3);
+}
+
+extern "C" int hh_solve_source_multi(hh_plan *const *plans, const int *nrhs, int nplans, const double *f, double *u) {
+    if (!plans || !nrhs || nplans < 1 || !f || !u) {
+        set_error("hh_solve_source_multi: invalid arguments");
+        return HH_ERR_INVALID;
+    }
+    long total = 0;
+    std::vector<Plan *> ps((size_t)nplans);
+    for (int i = 0; i < nplans; i++) {
+        if (!plans[i] || nrhs[i] < 0) { set_error("hh_solve_source_multi: plan %d or its count is invalid", i); return HH_ERR_INVALID; }
+        ps[(size_t)i] = &plans[i]->p;
+        const Plan &a = plans[0]->p, &b = plans[i]->p;
+        if (b.src_order == 0 || b.ctx != a.ctx || b.dim != a.dim || b.nx != a.nx || b.ny != a.ny || b.nz != a.nz ||
+            b.src_order != a.src_order) {
+            set_error("hh_solve_source_multi: plan %d is not a Helmholtz plan of plan 0's shape and context", i);
+            return HH_ERR_INVALID;
+        }
+        total += nrhs[i];
+    }
+    if (total > 65535) { set_error("hh_solve_source_multi: %ld right-hand sides", total); return HH_ERR_INVALID; }
+    HH_CUDA(cudaSetDevice(ps[0]->ctx->device));
+    return solve_source_multi(ps.data(), nrhs, nplans, (const double2 *)f, (double2 *)u, nullptr);
 }
 
 // Host buffers: the batch goes through in chunks so that the host-to-device copy of chunk i+1,

@@ -75,6 +75,7 @@ struct Ctx {
     int                     *err_word = nullptr; // set by kernels whose bounded waits expire
     int                     *inject_word = nullptr; // armed by hh_ctx_inject_wait_expiry, taken by one launch
     size_t                   l2_bytes = 0;        // the device's L2 size (3D transform slabs)
+    std::string              dev_name;            // the device's model name (tuning-cache key)
     // stage timing (hh_ctx_set_stage_timing)
     bool                     timing = false;
     std::vector<cudaEvent_t> ev_pending;          // groups of 4 events per timed solve
@@ -90,6 +91,9 @@ struct Ctx {
     unsigned long long      *norms = nullptr;
     double2                 *refine_work = nullptr;
     long                     refine_elems = 0;
+    // the chunk table of multi-plan solves (hh_solve_source_multi), grown on demand
+    void                    *multi_tab = nullptr;
+    size_t                   multi_tab_bytes = 0;
 };
 
 int tables_for(Ctx *c, int m, const double2 **tw, const double **sn);
@@ -138,6 +142,12 @@ int launch_dst_cols(Ctx *c, int n, long ncols, long planes, const double2 *in, l
                     double2 *out, bool lp = false, int kern = 0);
 int launch_factor(Plan *p, const double2 *subt, const double2 *diagt, const double2 *supt);
 int launch_line_solve(Plan *p, const double2 *in, double2 *out, int batch, int src_order);
+// one symmetric line-solve launch over several plans of one shape (plan i: nrhs[i] consecutive
+// fields); table_dev holds line_solve_multi_table_bytes(nplans, total) bytes; HH_ERR_UNSUPPORTED
+// (nothing launched) when the plans do not all take the same symmetric kernel variant
+size_t line_solve_multi_table_bytes(int nplans, int total);
+int launch_line_solve_multi(Plan *const *plans, const int *nrhs, int nplans, const double2 *in, double2 *out,
+                            int src_order, void *table_dev);
 // res = A_h u - rhs (FP64, zero Dirichlet ring); norms (optional, zeroed by the caller) receive
 // max |res| and max |rhs| over the batch as double bit patterns
 int launch_residual(Plan *p, const double2 *u, const double2 *rhs, double2 *res, int batch,
@@ -145,6 +155,9 @@ int launch_residual(Plan *p, const double2 *u, const double2 *rhs, double2 *res,
 int launch_axpy(Ctx *c, double2 *u, const double2 *v, double s, long n); // u += s v
 int read_device_error(Ctx *c, int *val);
 long slab_planes(const Plan &p, long planes); // 3D transform slab in planes (the plan's or the default)
+// the fused-source solve of several plans of one shape in one pass (hh_solve_source_multi);
+// table: device memory of line_solve_multi_table_bytes, or nullptr for the context's own
+int solve_source_multi(Plan *const *plans, const int *nrhs, int nplans, const double2 *f, double2 *u, void *table);
 int segment_count(int rows);
 int sym_default_variant(int rows);
 int padded_rows(int rows);

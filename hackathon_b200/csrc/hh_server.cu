@@ -7,14 +7,15 @@
 //    when the HBM budget needs the room; a new plan takes the kernel settings of its shape from
 //    the tuning cache (hh_plan_tune), if the process has tuned that shape;
 //  * continuous batching: when the dispatcher picks a request it also takes every queued request
-//    of the same plan (small ones, up to kMergeRhs right-hand sides in all) and runs them as one
-//    batched solve;
+//    of the same shape (dim, n, order) at any k (small ones, up to kMergeRhs right-hand sides in
+//    all) and runs them as one batched solve over several plans (one transform launch per
+//    direction, one line-solve launch with a table of which right-hand sides use which plan);
 //  * admission: a batch starts only while plans plus in-flight staging stay within the budget;
 //    otherwise it waits for running batches to finish;
 //  * batches go round-robin to several CUDA streams, so work of different requests overlaps on
 //    the device; completion is signalled by a host function enqueued behind each batch.
 // Every batched solve computes each right-hand side with exactly the arithmetic of a solo solve
-// on the same plan (the kernels never mix right-hand sides), so results are bitwise identical.
+// on its own plan (the kernels never mix right-hand sides), so results are bitwise identical.
 #include "hh_internal.cuh"
 
 #include <hh.h>
@@ -92,13 +93,16 @@ namespace {
 
 struct Batch {
     hh_server         *s = nullptr;
-    std::vector<Req *> reqs;
-    Key                key;
+    std::vector<Req *> reqs;             // grouped by plan: the requests of keys[i] are consecutive
+    std::vector<Key>   keys;             // the batch's plans (one per distinct k)
+    std::vector<int>   counts;           // right-hand sides per plan, in keys order
     size_t             staging = 0;
     bool               reserved = false; // staging counted in s->used
-    bool               plan_ref = false; // holds an in-flight reference on its plan
+    bool               plan_ref = false; // holds an in-flight reference on each of its plans
     int               *flag = nullptr;   // pinned copy of the device error word after the batch
 };
+
+Key key_of(const hh_request &r) { return Key{r.dim, r.n, r.order, r.k_re, r.k_im}; }
 
 long points_of(const hh_request &r) {
     long p = 1;
@@ -128,8 +132,10 @@ void batch_done(void *arg) {
         s->used -= b->staging;
         s->inflight--;
         s->completed += (long long)b->reqs.size();
-        auto it = s->plans.find(b->key);
-        if (it != s->plans.end()) it->second.inflight--;
+        for (const Key &k : b->keys) {
+            auto it = s->plans.find(k);
+            if (it != s->plans.end()) it->second.inflight--;
+        }
     }
     s->cv.notify_all();
     delete b;
@@ -148,10 +154,11 @@ void fail_batch(hh_server *s, Batch *b, int rc, const std::string &msg) {
         }
         if (b->reserved) s->used -= b->staging;
         s->inflight--;
-        if (b->plan_ref) {
-            auto it = s->plans.find(b->key);
-            if (it != s->plans.end()) it->second.inflight--;
-        }
+        if (b->plan_ref)
+            for (const Key &k : b->keys) {
+                auto it = s->plans.find(k);
+                if (it != s->plans.end()) it->second.inflight--;
+            }
     }
     s->cv.notify_all();
     delete b;
@@ -176,13 +183,16 @@ std::vector<hh_plan *> pick_victims(hh_server *s, size_t need) {
 }
 
 // Enqueue the batch on the next stream.  On failure nothing of it is left in flight.
-int run_batch(hh_server *s, Batch *b, hh_plan *plan, cudaEvent_t after) {
+int run_batch(hh_server *s, Batch *b, const std::vector<hh_plan *> &plans, cudaEvent_t after) {
     const hh_request &r0 = b->reqs[0]->r;
     const long        field = points_of(r0);
     const int         si = s->rr++ % (int)s->streams.size();
     cudaStream_t      st = s->streams[(size_t)si];
     double2          *buf = nullptr;
+    void             *tab = nullptr;
     hh::Ctx          *cx = reinterpret_cast<hh::Ctx *>(s->ctx); // Ctx is hh_ctx's first member
+    std::vector<hh::Plan *> ps;
+    for (hh_plan *pl : plans) ps.push_back(reinterpret_cast<hh::Plan *>(pl)); // Plan is hh_plan's first member
     bool              inject = false;
     {
         std::lock_guard<std::mutex> g(s->m);
@@ -198,8 +208,11 @@ int run_batch(hh_server *s, Batch *b, hh_plan *plan, cudaEvent_t after) {
         if (after) HH_CUDA(cudaStreamWaitEvent(st, after, 0)); // the plan's set-up
         int total = 0;
         for (Req *q : b->reqs) total += q->r.nrhs;
-        if (b->staging == 0) {
-            HH_TRY(hh_solve_source(plan, r0.f, r0.u, total)); // straight from the caller's device buffers
+        // the multi-plan chunk table of this batch, from the pool in stream order
+        HH_CUDA(cudaMallocFromPoolAsync(&tab, hh::line_solve_multi_table_bytes((int)ps.size(), total), s->pool, st));
+        if (b->staging == 0) { // straight from the caller's device buffers
+            HH_TRY(hh::solve_source_multi(ps.data(), b->counts.data(), (int)ps.size(), (const double2 *)r0.f,
+                                          (double2 *)r0.u, tab));
         } else {
             HH_CUDA(cudaMallocFromPoolAsync((void **)&buf, b->staging, s->pool, st));
             long off = 0;
@@ -209,7 +222,7 @@ int run_batch(hh_server *s, Batch *b, hh_plan *plan, cudaEvent_t after) {
                                         q->r.on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
                 off += field * q->r.nrhs;
             }
-            HH_TRY(hh_solve_source(plan, (const double *)buf, (double *)buf, total));
+            HH_TRY(hh::solve_source_multi(ps.data(), b->counts.data(), (int)ps.size(), buf, buf, tab));
             off = 0;
             for (Req *q : b->reqs) {
                 const size_t bytes = sizeof(double2) * (size_t)field * q->r.nrhs;
@@ -220,6 +233,8 @@ int run_batch(hh_server *s, Batch *b, hh_plan *plan, cudaEvent_t after) {
             HH_CUDA(cudaFreeAsync(buf, st));
             buf = nullptr;
         }
+        HH_CUDA(cudaFreeAsync(tab, st));
+        tab = nullptr;
         if (inject) HH_CUDA(cudaMemsetAsync(cx->err_word, 1, 1, st)); // as if a wait had expired
         b->flag = s->flags + si;
         HH_CUDA(cudaMemcpyAsync(b->flag, cx->err_word, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -230,6 +245,7 @@ int run_batch(hh_server *s, Batch *b, hh_plan *plan, cudaEvent_t after) {
     if (rc != HH_OK) {
         cudaStreamSynchronize(st); // copies already queued must not outlive the request
         if (buf) cudaFree(buf);
+        if (tab) cudaFree(tab);
     }
     return rc;
 }
@@ -243,31 +259,59 @@ void dispatcher(hh_server *s) {
             if (s->stop) break;
             continue;
         }
-        // the head request and every queued small request of the same plan (continuous batching)
+        // the head request and every queued small request of the same shape (dim, n, order), at any
+        // k: one batch over several plans (continuous batching)
         Req       *head = s->queue.front();
-        const Key  key{head->r.dim, head->r.n, head->r.order, head->r.k_re, head->r.k_im};
         const long field = points_of(head->r);
         Batch     *b = new Batch;
         b->s = s;
-        b->key = key;
-        b->reqs.push_back(head);
+        std::vector<Req *> picked{head};
         int rhs = head->r.nrhs;
         if (field * head->r.nrhs <= kMergePoints) {
             for (Req *q : s->queue) {
                 if (q == head || rhs >= kMergeRhs) continue;
-                const Key kq{q->r.dim, q->r.n, q->r.order, q->r.k_re, q->r.k_im};
-                if (kq == key && field * q->r.nrhs <= kMergePoints && rhs + q->r.nrhs <= kMergeRhs) {
-                    b->reqs.push_back(q);
+                if (q->r.dim == head->r.dim && q->r.n == head->r.n && q->r.order == head->r.order &&
+                    field * q->r.nrhs <= kMergePoints && rhs + q->r.nrhs <= kMergeRhs) {
+                    picked.push_back(q);
                     rhs += q->r.nrhs;
                 }
             }
         }
+        // group by plan (first appearance order), so that each plan's fields are consecutive
+        for (Req *q : picked) {
+            const Key k = key_of(q->r);
+            if (std::find(b->keys.begin(), b->keys.end(), k) == b->keys.end()) {
+                b->keys.push_back(k);
+                b->counts.push_back(0);
+            }
+        }
+        for (size_t i = 0; i < b->keys.size(); i++)
+            for (Req *q : picked)
+                if (key_of(q->r) == b->keys[i]) {
+                    b->reqs.push_back(q);
+                    b->counts[i] += q->r.nrhs;
+                }
         const bool direct = b->reqs.size() == 1 && head->r.on_device;
         b->staging = direct ? 0 : sizeof(double2) * (size_t)field * rhs;
-        auto need = [&]() { return b->staging + (s->plans.count(key) ? 0 : plan_bytes(head->r)); };
+        auto new_plan_bytes = [&]() {
+            size_t x = 0;
+            for (const Key &k : b->keys)
+                if (!s->plans.count(k)) x += plan_bytes(head->r);
+            return x;
+        };
+        auto need = [&]() { return b->staging + new_plan_bytes(); };
         // admission by HBM budget: wait for running batches, then evict idle plans
         while (s->used + need() > s->budget && s->inflight > 0) s->cv.wait(lk);
+        // plans of this batch are not victims: hold them while evicting
+        for (const Key &k : b->keys) {
+            auto it = s->plans.find(k);
+            if (it != s->plans.end()) it->second.inflight++;
+        }
         std::vector<hh_plan *> victims = pick_victims(s, need());
+        for (const Key &k : b->keys) {
+            auto it = s->plans.find(k);
+            if (it != s->plans.end()) it->second.inflight--;
+        }
         if (!victims.empty()) {
             lk.unlock();
             hh_ctx_set_stream(s->ctx, s->setup); // idle plans: their memory returns to the pool in order
@@ -281,8 +325,10 @@ void dispatcher(hh_server *s) {
             q->info.batch_rhs = rhs;
         }
         s->inflight++;
-        const bool   create = s->plans.count(key) == 0;
-        const size_t pbytes = create ? plan_bytes(head->r) : 0;
+        std::vector<Key> create;
+        for (const Key &k : b->keys)
+            if (!s->plans.count(k)) create.push_back(k);
+        const size_t pbytes = create.size() * plan_bytes(head->r);
         if (s->used + b->staging + pbytes > s->budget) {
             lk.unlock();
             fail_batch(s, b, HH_ERR_NOMEM, "request does not fit in the server's HBM budget");
@@ -291,21 +337,28 @@ void dispatcher(hh_server *s) {
         }
         s->used += b->staging + pbytes; // staging and (reserved) plan memory
         b->reserved = true;
-        hh_plan *plan = nullptr;
         bool fresh = false;
-        if (create) {
+        if (!create.empty()) {
             lk.unlock();
             // asynchronous set-up on its own stream; the batch waits for it with an event
-            const hh_request &r = head->r;
             int rc = hh_ctx_set_stream(s->ctx, s->setup);
-            if (rc == HH_OK)
-                rc = r.dim == 2 ? hh_plan2d_create_helmholtz(s->ctx, r.n, r.order, r.k_re, r.k_im, &plan)
-                                : hh_plan3d_create_helmholtz(s->ctx, r.n, r.order, r.k_re, r.k_im, &plan);
-            int tuned = 0; // the kernel settings hh_plan_tune found for this shape, if any (never measures)
-            if (rc == HH_OK) rc = hh_plan_apply_tuning(plan, &tuned);
+            std::vector<hh_plan *> made;
+            for (const Key &k : create) {
+                if (rc != HH_OK) break;
+                const int dim = std::get<0>(k), n = std::get<1>(k), order = std::get<2>(k);
+                const double kr = std::get<3>(k), ki = std::get<4>(k);
+                hh_plan *plan = nullptr;
+                rc = dim == 2 ? hh_plan2d_create_helmholtz(s->ctx, n, order, kr, ki, &plan)
+                              : hh_plan3d_create_helmholtz(s->ctx, n, order, kr, ki, &plan);
+                int tuned = 0; // the kernel settings hh_plan_tune found for this shape, if any (never measures)
+                if (rc == HH_OK) rc = hh_plan_apply_tuning(plan, &tuned);
+                if (plan) made.push_back(plan);
+            }
             if (rc == HH_OK && cudaEventRecord(s->ready, s->setup) != cudaSuccess) rc = HH_ERR_CUDA;
             const std::string msg = rc == HH_OK ? std::string() : std::string(hh_last_error());
             fresh = rc == HH_OK;
+            if (rc != HH_OK)
+                for (hh_plan *pl : made) hh_plan_destroy(pl);
             lk.lock();
             if (rc != HH_OK) {
                 s->used -= pbytes;
@@ -314,18 +367,23 @@ void dispatcher(hh_server *s) {
                 lk.lock();
                 continue;
             }
-            PlanEntry e;
-            e.plan = plan;
-            e.bytes = pbytes;
-            s->plans.emplace(key, e);
+            for (size_t i = 0; i < create.size(); i++) {
+                PlanEntry e;
+                e.plan = made[i];
+                e.bytes = plan_bytes(head->r);
+                s->plans.emplace(create[i], e);
+            }
         }
-        PlanEntry &pe = s->plans[key];
-        pe.inflight++;
-        pe.last_use = ++s->tick;
-        plan = pe.plan;
+        std::vector<hh_plan *> plans;
+        for (const Key &k : b->keys) {
+            PlanEntry &pe = s->plans[k];
+            pe.inflight++;
+            pe.last_use = ++s->tick;
+            plans.push_back(pe.plan);
+        }
         b->plan_ref = true;
         lk.unlock();
-        const int rc = run_batch(s, b, plan, fresh ? s->ready : nullptr);
+        const int rc = run_batch(s, b, plans, fresh ? s->ready : nullptr);
         if (rc != HH_OK) fail_batch(s, b, rc, hh_last_error());
         lk.lock();
     }

@@ -1044,12 +1044,24 @@ __host__ __device__ inline int sym_tile_elems(int rows, int cw) {
     return (nbox * br * cw + 7) / 8 * 8;
 }
 
+// Several plans of one shape in one launch (hh_solve_source_multi): chunk j of the grid's y
+// dimension solves right-hand sides [b0, b1) of the batch with the factors and wavenumber of plan
+// `plan`; everything else (eigenvalues, Pade factors, h) is the same for plans of one shape.
+struct SymPlanRef {
+    const double2 *Pv, *subt, *diagt;
+    double2        k2h2_20;
+};
+struct SymChunk {
+    int plan, b0, b1, pad;
+};
+
 template <int SRC, int NT, int CW, int MINB, int NR, int KS, bool TIO>
 __global__ void __launch_bounds__(NT, MINB)
     k_line_solve_sym(const double2 *__restrict__ in, double2 *__restrict__ out, int lines, int rows, long row_stride,
-                     long field, int batch, int rb, const double2 *__restrict__ Pv, const double2 *__restrict__ subt,
-                     const double2 *__restrict__ diagt, int prow, const double *__restrict__ mu, SymParams sp,
-                     const __grid_constant__ CUtensorMap in_map, int *err) {
+                     long field, int batch, int rb, const double2 *__restrict__ Pv_one, const double2 *__restrict__ subt_one,
+                     const double2 *__restrict__ diagt_one, int prow, const double *__restrict__ mu, SymParams sp,
+                     const __grid_constant__ CUtensorMap in_map, int *err, const SymPlanRef *__restrict__ refs,
+                     const SymChunk *__restrict__ chunks) {
     constexpr int NW = NT / 32, SPW = 32 / CW, LOG = ilog2_t<SPW>();
     constexpr int HALO = (SRC == 4 || SRC == 6) ? 1 : 0;
     __shared__ SymSmem<NW, CW, NR> sm;
@@ -1070,6 +1082,22 @@ __global__ void __launch_bounds__(NT, MINB)
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const int c = t % CW, seg = t / CW, sl = lane / CW;
     const int q = blockIdx.x * CW + c;
+    // this CTA's right-hand sides and the plan they belong to
+    int            b_begin, b_end;
+    const double2 *Pv = Pv_one, *subt = subt_one, *diagt = diagt_one;
+    if (chunks) {
+        const SymChunk   ch = chunks[blockIdx.y];
+        const SymPlanRef pr = refs[ch.plan];
+        b_begin = ch.b0;
+        b_end = ch.b1;
+        Pv = pr.Pv;
+        subt = pr.subt;
+        diagt = pr.diagt;
+        sp.k2h2_20 = pr.k2h2_20;
+    } else {
+        b_begin = blockIdx.y * rb;
+        b_end = min(batch, b_begin + rb);
+    }
     SymTio    tio{};
     if constexpr (TIO) {
         constexpr int NBUF = SymTileBufs<SRC>::value;
@@ -1083,7 +1111,7 @@ __global__ void __launch_bounds__(NT, MINB)
         tio.tile = sym_tile_elems(rows, CW);
         tio.tile_bytes = (unsigned)(tio.nbox * tio.br * CW * 16);
         if (t == 0) { // the first right-hand sides' tiles come in while the factors are set up
-            const int b0 = blockIdx.y * rb, b1 = min(batch, b0 + rb);
+            const int b0 = b_begin, b1 = b_end;
             for (int u = 0; u < NBUF; u++) mbar_init(tio.bar + u, 1);
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
             for (int u = 0; u < NBUF && b0 + u < b1; u++) {
@@ -1181,8 +1209,6 @@ __global__ void __launch_bounds__(NT, MINB)
     }
     __syncthreads();
 
-    const int  b_begin = blockIdx.y * rb;
-    const int  b_end = min(batch, b_begin + rb);
     const long off0 = (long)r0 * row_stride + qq;
     // warps whose rows all lie in [9, rows) use the constant Pade factors
     const bool tint = (w * SPW * KS >= 9) && ((w + 1) * SPW * KS <= rows);
@@ -1223,8 +1249,16 @@ static int encode_line_map(CUtensorMap *map, const double2 *base, const Plan *p,
     return encode_tensor_map(map, base, 4, dims, strides, box);
 }
 
+// A multi-plan launch: the plans' references and the chunk table, in device memory the caller
+// provides, and the chunk count (the grid's y extent).
+struct SymMulti {
+    const SymPlanRef *refs = nullptr;
+    const SymChunk   *chunks = nullptr;
+    int               nchunks = 0;
+};
+
 template <int SRC, int CW, int MINB, int NR, int KS, bool TIO>
-static int launch_sym_t(Plan *p, const double2 *in, double2 *out, int batch) {
+static int launch_sym_t(Plan *p, const double2 *in, double2 *out, int batch, const SymMulti *multi) {
     constexpr int NT = 256, SPW = 32 / CW, LOG = ilog2_t<SPW>();
     SymParams sp;
     sp.h2 = p->h * p->h;
@@ -1249,11 +1283,11 @@ static int launch_sym_t(Plan *p, const double2 *in, double2 *out, int batch) {
     HH_CUDA(cudaGetDevice(&dev));
     HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int rb = pick_rb(groups, batch, std::max(1, blocks_per_sm) * sms, NR);
-    const int chunks = (batch + rb - 1) / rb;
+    const int chunks = multi ? multi->nchunks : (batch + rb - 1) / rb;
     dim3 grid((unsigned)groups, (unsigned)chunks);
     k_line_solve_sym<SRC, NT, CW, MINB, NR, KS, TIO><<<grid, NT, shm, p->ctx->stream>>>(
         in, out, p->lines, p->rows, p->row_stride, p->field, batch, rb, p->Pv, p->subt, p->diagt, p->prow, p->mu, sp,
-        in_map, p->ctx->err_word);
+        in_map, p->ctx->err_word, multi ? multi->refs : nullptr, multi ? multi->chunks : nullptr);
     HH_CUDA(cudaGetLastError());
     p->ctx->launches++;
     return HH_OK;
@@ -1261,18 +1295,23 @@ static int launch_sym_t(Plan *p, const double2 *in, double2 *out, int batch) {
 
 // TIO: tile I/O where a line group is at least four lines (64-byte row pieces); narrower groups
 // keep the per-thread prefetch.
-template <int SRC, int MINB, int NR, int KS, bool TIO = false>
-static int launch_sym_src(Plan *p, const double2 *in, double2 *out, int batch) {
-    // segments per line: a power of two P >= rows / KS with 8 <= P <= 256 (CW = 256 / P lines per CTA)
+// segments per line of the symmetric kernel: a power of two P >= rows / KS with 8 <= P <= 256
+// (CW = 256 / P lines per CTA); P = 8 runs one right-hand side per pass
+static int sym_segments(int rows, int ks) {
     int P = 8;
-    while (P * KS < p->rows) P <<= 1;
-    switch (P) {
-    case 8: return launch_sym_t<SRC, 32, MINB, 1, KS, TIO>(p, in, out, batch); // per-RHS scan arrays would not fit
-    case 16: return launch_sym_t<SRC, 16, MINB, NR, KS, TIO>(p, in, out, batch);
-    case 32: return launch_sym_t<SRC, 8, MINB, NR, KS, TIO>(p, in, out, batch);
-    case 64: return launch_sym_t<SRC, 4, MINB, NR, KS, TIO>(p, in, out, batch);
-    case 128: return launch_sym_t<SRC, 2, MINB, NR, KS, false>(p, in, out, batch);
-    case 256: return launch_sym_t<SRC, 1, MINB, NR, KS, false>(p, in, out, batch);
+    while (P * ks < rows) P <<= 1;
+    return P;
+}
+
+template <int SRC, int MINB, int NR, int KS, bool TIO = false>
+static int launch_sym_src(Plan *p, const double2 *in, double2 *out, int batch, const SymMulti *multi) {
+    switch (sym_segments(p->rows, KS)) {
+    case 8: return launch_sym_t<SRC, 32, MINB, 1, KS, TIO>(p, in, out, batch, multi); // per-RHS scan arrays would not fit
+    case 16: return launch_sym_t<SRC, 16, MINB, NR, KS, TIO>(p, in, out, batch, multi);
+    case 32: return launch_sym_t<SRC, 8, MINB, NR, KS, TIO>(p, in, out, batch, multi);
+    case 64: return launch_sym_t<SRC, 4, MINB, NR, KS, TIO>(p, in, out, batch, multi);
+    case 128: return launch_sym_t<SRC, 2, MINB, NR, KS, false>(p, in, out, batch, multi);
+    case 256: return launch_sym_t<SRC, 1, MINB, NR, KS, false>(p, in, out, batch, multi);
     default: set_error("symmetric line solve: %d rows", p->rows); return HH_ERR_UNSUPPORTED;
     }
 }
@@ -1291,24 +1330,83 @@ bool sym_solve_supported(const Plan *p, int src_order) {
 // (twice the lines per CTA: wider contiguous row pieces in global memory, half the scans; at
 // order 6 the reciprocal pivots move to shared memory), 6 = variant 5 with each right-hand side
 // brought in as a TMA tile where a CTA holds at least four lines.
-template <int SRC> static int launch_sym_variant(Plan *p, const double2 *in, double2 *out, int batch) {
+template <int SRC>
+static int launch_sym_variant(Plan *p, const double2 *in, double2 *out, int batch, const SymMulti *multi) {
     switch (p->variant) {
-    case 3: return launch_sym_src<SRC, 1, 1, kSeg>(p, in, out, batch);
-    case 4: return launch_sym_src<SRC, 1, 2, kSeg>(p, in, out, batch);
-    case 5: return launch_sym_src<SRC, 1, 1, 16>(p, in, out, batch);
-    case 6: return launch_sym_src<SRC, 1, 1, 16, true>(p, in, out, batch);
-    default: return launch_sym_src<SRC, 2, 1, kSeg>(p, in, out, batch);
+    case 3: return launch_sym_src<SRC, 1, 1, kSeg>(p, in, out, batch, multi);
+    case 4: return launch_sym_src<SRC, 1, 2, kSeg>(p, in, out, batch, multi);
+    case 5: return launch_sym_src<SRC, 1, 1, 16>(p, in, out, batch, multi);
+    case 6: return launch_sym_src<SRC, 1, 1, 16, true>(p, in, out, batch, multi);
+    default: return launch_sym_src<SRC, 2, 1, kSeg>(p, in, out, batch, multi);
+    }
+}
+
+static int launch_sym_order(Plan *p, const double2 *in, double2 *out, int batch, int src_order, const SymMulti *multi) {
+    switch (src_order) {
+    case 0: return launch_sym_variant<0>(p, in, out, batch, multi);
+    case 2: return launch_sym_variant<2>(p, in, out, batch, multi);
+    case 4: return launch_sym_variant<4>(p, in, out, batch, multi);
+    case 6: return launch_sym_variant<6>(p, in, out, batch, multi);
+    default: set_error("source operator order %d", src_order); return HH_ERR_INVALID;
     }
 }
 
 int launch_line_solve_sym(Plan *p, const double2 *in, double2 *out, int batch, int src_order) {
-    switch (src_order) {
-    case 0: return launch_sym_variant<0>(p, in, out, batch);
-    case 2: return launch_sym_variant<2>(p, in, out, batch);
-    case 4: return launch_sym_variant<4>(p, in, out, batch);
-    case 6: return launch_sym_variant<6>(p, in, out, batch);
-    default: set_error("source operator order %d", src_order); return HH_ERR_INVALID;
+    return launch_sym_order(p, in, out, batch, src_order, nullptr);
+}
+
+size_t line_solve_multi_table_bytes(int nplans, int total) {
+    return sizeof(SymPlanRef) * (size_t)nplans + sizeof(SymChunk) * (size_t)(total + nplans);
+}
+
+// One symmetric line-solve launch over the right-hand sides of several plans of one shape: plan i
+// solves nrhs[i] consecutive fields of the batch (plans in order).  Every plan must take the
+// symmetric kernel with the same variant; table_dev (line_solve_multi_table_bytes) receives the
+// plan references and the chunk table in stream order.  Returns HH_ERR_UNSUPPORTED when the plans
+// do not qualify, before launching anything.
+int launch_line_solve_multi(Plan *const *plans, const int *nrhs, int nplans, const double2 *in, double2 *out,
+                            int src_order, void *table_dev) {
+    Plan *p0 = plans[0];
+    for (int i = 0; i < nplans; i++) {
+        const Plan *pi = plans[i];
+        if (pi->variant < 2 || pi->variant != p0->variant || !sym_solve_supported(pi, src_order)) {
+            set_error("multi-plan line solve: plan %d does not take the symmetric kernel variant %d", i, p0->variant);
+            return HH_ERR_UNSUPPORTED;
+        }
     }
+    int total = 0;
+    for (int i = 0; i < nplans; i++) total += nrhs[i];
+    if (total == 0) return HH_OK;
+    // right-hand sides per chunk: the single-plan choice for the whole batch, chunks never
+    // crossing a plan boundary
+    const int ks = (p0->variant >= 5) ? 16 : kSeg;
+    const int P = sym_segments(p0->rows, ks), CW = 256 / P, nr = (p0->variant == 4 && P > 8) ? 2 : 1;
+    const long groups = (p0->lines + CW - 1) / CW;
+    int dev = 0, sms = 148;
+    HH_CUDA(cudaGetDevice(&dev));
+    HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int rb = pick_rb(groups, total, (p0->variant == 2 ? 2 : 1) * sms, nr);
+    std::vector<SymPlanRef> refs((size_t)nplans);
+    std::vector<SymChunk>   chunks;
+    for (int i = 0, b = 0; i < nplans; b += nrhs[i], i++) {
+        const Plan *pi = plans[i];
+        const double h2 = pi->h * pi->h;
+        refs[(size_t)i] = SymPlanRef{pi->Pv, pi->subt, pi->diagt, make_double2(pi->k2.x * h2 / 20.0, pi->k2.y * h2 / 20.0)};
+        for (int b0 = b; b0 < b + nrhs[i]; b0 += rb) chunks.push_back(SymChunk{i, b0, std::min(b + nrhs[i], b0 + rb), 0});
+    }
+    if (chunks.size() > 65535) {
+        set_error("multi-plan line solve: %zu chunks", chunks.size());
+        return HH_ERR_UNSUPPORTED;
+    }
+    char *tab = static_cast<char *>(table_dev);
+    HH_CUDA(cudaMemcpyAsync(tab, refs.data(), sizeof(SymPlanRef) * refs.size(), cudaMemcpyHostToDevice, p0->ctx->stream));
+    HH_CUDA(cudaMemcpyAsync(tab + sizeof(SymPlanRef) * refs.size(), chunks.data(), sizeof(SymChunk) * chunks.size(),
+                            cudaMemcpyHostToDevice, p0->ctx->stream));
+    SymMulti m;
+    m.refs = reinterpret_cast<const SymPlanRef *>(tab);
+    m.chunks = reinterpret_cast<const SymChunk *>(tab + sizeof(SymPlanRef) * refs.size());
+    m.nchunks = (int)chunks.size();
+    return launch_sym_order(p0, in, out, total, src_order, &m);
 }
 
 } // namespace hh

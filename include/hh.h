@@ -162,6 +162,17 @@ int hh_solve_host(hh_plan *plan, const double *rhs_host, double *sol_host, int b
  * 2D_Program/main_functions/rhs.c:100, 3D_Program/main_functions/rhs.c:198, for this class). */
 int hh_solve_source(hh_plan *plan, const double *f_dev, double *u_dev, int batch);
 int hh_solve_source_host(hh_plan *plan, const double *f_host, double *u_host, int batch);
+/* Several wavenumbers in one solve (no counterpart in the reference, which solves one k per
+ * run): nplans Helmholtz plans of one shape (dim, n, order) on one context, plan i taking the
+ * nrhs[i] consecutive fields of f_dev and u_dev that follow those of plans 0..i-1.  The transforms
+ * do not depend on k, so each direction is one launch over the whole batch; where every plan takes
+ * the same symmetric line-solve variant (set by hh_plan_set_variant, or hh_plan_tune / the tuning
+ * cache, which give plans of one shape the same one) the line solves are one launch as well, with
+ * a table of which right-hand sides use which plan's factors; otherwise one line-solve launch per
+ * plan.  Each field gets exactly the arithmetic of hh_solve_source on its own plan.  The table
+ * lives in a context buffer grown on demand (allocation outside stream capture). */
+int hh_solve_source_multi(hh_plan *const *plans, const int *nrhs, int nplans, const double *f_dev, double *u_dev);
+
 /* The same host-buffer solve without any allocation (no counterpart in the reference).  For
  * callers that must not allocate device memory while they run, e.g. with a fixed memory budget
  * or where allocator latency is unwelcome: the device staging is a 32 MiB array of the library
@@ -205,8 +216,9 @@ int hh_coefficients3d(int n, int order, double k_re, double k_im, double *const 
  *  - one plan per (dim, n, order, k) stays resident (least recently used plans are evicted
  *    when the HBM budget needs the room); new plans take the tuning cache's settings for their
  *    shape (hh_plan_apply_tuning), so tune one plan per served shape beforehand;
- *  - continuous batching: queued requests of the same plan (up to 64 right-hand sides, each
- *    request at most 4M points) run as one batched solve;
+ *  - continuous batching: queued requests of the same shape (dim, n, order) at any k (up to 64
+ *    right-hand sides, each request at most 4M points) run as one batched solve over their plans
+ *    (hh_solve_source_multi);
  *  - admission: a batch starts while plans plus in-flight staging fit the HBM budget, otherwise
  *    it waits for running batches; a request that can never fit fails with HH_ERR_NOMEM;
  *  - batches go round-robin to `streams` CUDA streams, so requests overlap on the device.

@@ -36,6 +36,7 @@ def test_expired_wait_fails_its_request_in_the_loop(ctx):
     rng = np.random.default_rng(6)
     f = rng.standard_normal((nrhs, n, n)) + 1j * rng.standard_normal((nrhs, n, n))
     plan = hh.Plan.helmholtz(ctx, 2, n, 6, 12.0)
+    plan.apply_tuning()  # the settings the request loop's plan of this shape takes
     solo = plan.solve_source_host(f)
     plan.close()
     srv = hh.Server(0, hbm_budget=2 << 30, streams=2)

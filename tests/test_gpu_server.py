@@ -1,5 +1,6 @@
 """The request loop (include/hh.h hh_server_*): a mixed stream of 2D/3D requests, merged into
-batches and spread over streams, gives every request exactly the result of a solo solve."""
+batches (requests of one shape at any k share a batch) and spread over streams, gives every
+request exactly the result of a solo solve."""
 import numpy as np
 import pytest
 
@@ -25,7 +26,10 @@ def _requests(seed, count):
 
 
 def _solo(ctx, dim, n, order, k, f):
+    """The request alone: a plan of its own with the kernel settings the request loop's plans take
+    (the tuning cache's entry for the shape, if the process has one)."""
     plan = hh.Plan.helmholtz(ctx, dim, n, order, k)
+    plan.apply_tuning()
     u = plan.solve_source_host(f)
     plan.close()
     return u

@@ -292,3 +292,40 @@ def test_tile_io_short_lines_every_variant(ctx, dim, n, order):
         assert rel_err(outs[v], outs[5]) < TOL
     assert np.array_equal(outs[6], outs[5])
     plan.close()
+
+
+@pytest.mark.parametrize("dim,n,order,variant", [(2, 255, 6, 6), (2, 1023, 4, 6), (2, 127, 2, 4), (3, 63, 6, 5),
+                                                 (3, 31, 4, 6), (2, 2047, 6, 5), (2, 511, 6, 0)])
+def test_several_wavenumbers_in_one_solve(ctx, dim, n, order, variant):
+    """hh_solve_source_multi: plans of one shape at different k share the transform launches and
+    (same symmetric variant) one line-solve launch; each field is bitwise the solo solve of its own
+    plan.  Variant 0 (the general kernel) takes the one-launch-per-plan path."""
+    torch = pytest.importorskip("torch")
+    ks, counts = [7.0, 33.3 + 1.5j, 120.0], [3, 1, 2]
+    g = torch.Generator().manual_seed(n + order)
+    shape = (sum(counts),) + (n,) * dim
+    f = torch.complex(torch.randn(shape, generator=g, dtype=torch.float64),
+                      torch.randn(shape, generator=g, dtype=torch.float64)).cuda()
+    plans = [hh.Plan.helmholtz(ctx, dim, n, order, k) for k in ks]
+    for p in plans:
+        p.variant = variant
+    u = torch.full_like(f, float("nan"))
+    before = ctx.launches
+    hh.solve_source_multi(plans, counts, f, u)
+    ctx.synchronize()
+    launches = ctx.launches - before
+    per_dir = 1 if dim == 2 else 2
+    assert launches == 2 * per_dir + (1 if variant >= 2 else len(ks))
+    got = u.cpu().numpy()
+    off = 0
+    for p, c in zip(plans, counts):
+        solo = torch.empty_like(f[off:off + c])
+        p.solve_source(f[off:off + c], solo, c)
+        ctx.synchronize()
+        assert np.array_equal(got[off:off + c], solo.cpu().numpy())
+        off += c
+    with pytest.raises(hh.HHError):
+        other = hh.Plan.helmholtz(ctx, dim, n, 2 if order != 2 else 4, 10.0)
+        hh.solve_source_multi([plans[0], other], [1, 1], f, u)
+    for p in plans:
+        p.close()
