@@ -268,10 +268,21 @@ void dispatcher(hh_server *s) {
         std::vector<Req *> picked{head};
         int rhs = head->r.nrhs;
         if (field * head->r.nrhs <= kMergePoints) {
+            // a merged batch never needs more than the whole budget on its own: its staging plus
+            // the plans it would create
+            std::vector<Key> seen{key_of(head->r)};
+            int fresh_plans = s->plans.count(seen[0]) ? 0 : 1;
             for (Req *q : s->queue) {
                 if (q == head || rhs >= kMergeRhs) continue;
                 if (q->r.dim == head->r.dim && q->r.n == head->r.n && q->r.order == head->r.order &&
                     field * q->r.nrhs <= kMergePoints && rhs + q->r.nrhs <= kMergeRhs) {
+                    const Key  kq = key_of(q->r);
+                    const bool add_key = std::find(seen.begin(), seen.end(), kq) == seen.end();
+                    const int  fp = fresh_plans + (add_key && !s->plans.count(kq) ? 1 : 0);
+                    const size_t need_q = sizeof(double2) * (size_t)field * (rhs + q->r.nrhs) + fp * plan_bytes(head->r);
+                    if (need_q > s->budget) continue;
+                    if (add_key) seen.push_back(kq);
+                    fresh_plans = fp;
                     picked.push_back(q);
                     rhs += q->r.nrhs;
                 }
