@@ -223,6 +223,32 @@ def cpu_check_secondary() -> dict:
     return out
 
 
+def reference_gpu_3d(n: int = 127, reps: int = 4) -> dict:
+    """The reference's own 3D GPU solver (its cuFFT + CUDA-kernel solver() built unchanged into
+    oracle/_ref/time3d_gpu) beside the drop-in (the same harness linked against libhh3d.so,
+    oracle/_ref/time3d_hh): the reference's main() call sequence on its own problem, order 6, with
+    solver() timed by wall clock `reps` times (host data in, solution back on the host).  Calls
+    after the first are reported; each program prints its error against the analytic solution."""
+    import re
+    out = {"grid": f"{n}^3", "order": 6, "timing": "wall clock per solver() call, calls 2..reps"}
+    for name, exe in (("reference_gpu_solver", "time3d_gpu"), ("dropin_solver", "time3d_hh")):
+        path = os.path.join(ROOT, "oracle", "_ref", exe)
+        if not os.path.exists(path):
+            out[name] = {"unavailable": f"{exe} not built (make -C oracle gpu)"}
+            continue
+        try:
+            r = subprocess.run([path, "6", str(n), str(n), str(n)], capture_output=True, text=True, timeout=300,
+                               env=dict(os.environ, HH_REPS=str(reps)))
+        except Exception as e:  # a comparison point only
+            out[name] = {"unavailable": str(e)[:200]}
+            continue
+        walls = [float(x) for x in re.findall(r"solver call \d+: wall ([0-9.eE+-]+) s", r.stdout)]
+        err = re.findall(r"\|\|error\|\|_inf = ([0-9.eE+-]+)", r.stdout)
+        out[name] = {"rc": r.returncode, "first_call_s": walls[0] if walls else None,
+                     "later_calls_s": walls[1:], "error_inf": float(err[0]) if err else None}
+    return out
+
+
 def accuracy_vs_exact(gpu_solve) -> dict:
     """Error of the benchmarked solve against the manufactured exact solution: the first
     right-hand side of every (order, k) without its noise term (the noise has no closed-form
@@ -683,6 +709,7 @@ def main():
             line["accuracy"]["max_rel_err_vs_oracle"] = max(vs.values()) if vs else None
             if "secondary" in line:
                 line["cpu_baseline"]["secondary"] = cpu_check_secondary()
+                line["cpu_baseline"]["reference_gpu_path_3d"] = reference_gpu_3d()
         line["accuracy"]["max_rel_err_vs_exact"] = max(line["accuracy"]["rel_err_vs_exact_noise_free_rhs"].values())
         print(json.dumps(line), flush=True)
     for p in plans:

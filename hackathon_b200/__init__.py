@@ -39,6 +39,19 @@ class RequestInfo(C.Structure):
                 ("batch_rhs", C.c_int)]
 
 
+class Rhs2DData(C.Structure):
+    """include/hh.h hh_rhs2d_data"""
+    _fields_ = [("order", C.c_int), ("hx", C.c_double), ("hy", C.c_double)] + \
+               [(nm, C.c_void_p) for nm in ("f_ext", "k_ext", "k2y_bc", "fxx_xb", "fxx_yb", "fyy_xb", "fyy_yb",
+                                            "fy_yb", "u_xb", "u_yb")]
+
+
+class Rhs3DData(C.Structure):
+    """include/hh.h hh_rhs3d_data"""
+    _fields_ = [("order", C.c_int), ("hx", C.c_double), ("hy", C.c_double), ("hz", C.c_double)] + \
+               [(nm, C.c_void_p) for nm in ("f_ext", "k2_ext", "kz_bc", "fxx_b", "fyy_b", "fzz_b", "ue_ext")]
+
+
 SIGNATURES = {
     "hh_last_error": (C.c_char_p, []),
     "hh_version": (_i, []),
@@ -79,6 +92,8 @@ SIGNATURES = {
     "hh_solve_source_host": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source_host_noalloc": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source_multi": (_i, [C.POINTER(_vp), C.POINTER(_i), _i, _vp, _vp]),
+    "hh_rhs2d": (_i, [_vp, C.POINTER(Rhs2DData), _vp]),
+    "hh_rhs3d": (_i, [_vp, C.POINTER(Rhs3DData), _vp]),
     "hh_residual": (_i, [_vp, _vp, _vp, _vp, _i, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "hh_solve_refined": (_i, [_vp, _vp, _vp, _i, C.c_double, _i, C.POINTER(_i), C.POINTER(C.c_double)]),
     "hh_coefficients2d": (_i, [_i, _i, _d, _d, C.POINTER(_vp)]),
@@ -294,6 +309,33 @@ class Plan:
         check(lib().hh_solve_refined(self.h, _addr(rhs), _addr(sol), batch, tol, max_iter, C.byref(it), C.byref(rr)),
               "hh_solve_refined")
         return it.value, rr.value
+
+    def assemble_rhs(self, rhs, order: int, h, **data):
+        """hh_rhs2d / hh_rhs3d: the reference's rhs() on the device into the device buffer rhs.
+        h: (hx, hy) or (hx, hy, hz).  data: the hh_rhs{2,3}d_data arrays by name -- device buffers
+        (torch tensors or addresses), except k_ext / k2y_bc / k2_ext / kz_bc, which are host numpy
+        arrays; missing boundary arrays are zero."""
+        keep = []
+
+        def ptr(name, v):
+            if v is None:
+                return None
+            if name in ("k_ext", "k2y_bc", "k2_ext", "kz_bc"):
+                a = np.ascontiguousarray(v, dtype=np.complex128)
+                keep.append(a)
+                return a.ctypes.data
+            return _addr(v)
+
+        if self.dim == 2:
+            d = Rhs2DData(order, *h)
+            for nm, _ in Rhs2DData._fields_[3:]:
+                setattr(d, nm, ptr(nm, data.get(nm)))
+            check(lib().hh_rhs2d(self.h, C.byref(d), _addr(rhs)), "hh_rhs2d")
+        else:
+            d = Rhs3DData(order, *h)
+            for nm, _ in Rhs3DData._fields_[4:]:
+                setattr(d, nm, ptr(nm, data.get(nm)))
+            check(lib().hh_rhs3d(self.h, C.byref(d), _addr(rhs)), "hh_rhs3d")
 
     def residual(self, sol, rhs, res, batch: int = 1, norms: bool = False):
         """hh_residual on device buffers: res = A_h sol - rhs; with norms, (max|res|, max|rhs|)."""

@@ -26,7 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"] + ARCH
 CC_FLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall"]
 
-CU_SOURCES = ["hh_api.cu", "hh_dst.cu", "hh_tridiag.cu", "hh_server.cu", "hh_refine.cu"]
+CU_SOURCES = ["hh_api.cu", "hh_dst.cu", "hh_tridiag.cu", "hh_server.cu", "hh_refine.cu", "hh_rhs.cu"]
 C_SOURCES = ["hh_coef.c"]
 HEADERS = ["hh_internal.cuh", "hh_tma.cuh"]
 

@@ -145,6 +145,8 @@ extern "C" int hh_ctx_destroy(hh_ctx *x) {
     cudaFree(x->c.norms);
     cudaFree(x->c.refine_work);
     cudaFree(x->c.multi_tab);
+    cudaFree(x->c.rhs_work);
+    cudaFree(x->c.rhs_tab);
     cudaFree(x->stage);
     for (cudaEvent_t e : x->c.chunk_ev) cudaEventDestroy(e);
     if (x->c.copy_in) cudaStreamDestroy(x->c.copy_in);
@@ -1040,6 +1042,29 @@ extern "C" int hh_solve_source_multi(hh_plan *const *plans, const int *nrhs, int
     if (total > 65535) { set_error("hh_solve_source_multi: %ld right-hand sides", total); return HH_ERR_INVALID; }
     HH_CUDA(cudaSetDevice(ps[0]->ctx->device));
     return solve_source_multi(ps.data(), nrhs, nplans, (const double2 *)f, (double2 *)u, nullptr);
+}
+
+extern "C" int hh_rhs2d(hh_plan *pl, const hh_rhs2d_data *d, double *rhs) {
+    if (!pl || !d || !rhs || !d->f_ext || pl->p.dim != 2 || (d->order != 2 && d->order != 4 && d->order != 6) ||
+        (d->order == 6 && !d->k_ext) || pl->p.nx < 3 || pl->p.ny < 3 || !(d->hx > 0.0) || !(d->hy > 0.0)) {
+        set_error("hh_rhs2d: invalid arguments (a 2D plan of at least 3 x 3 points, order 2/4/6, f_ext, k_ext "
+                  "for order 6, positive spacings)");
+        return HH_ERR_INVALID;
+    }
+    HH_CUDA(cudaSetDevice(pl->p.ctx->device));
+    return assemble_rhs2d(&pl->p, d, (double2 *)rhs);
+}
+
+extern "C" int hh_rhs3d(hh_plan *pl, const hh_rhs3d_data *d, double *rhs) {
+    if (!pl || !d || !rhs || !d->f_ext || pl->p.dim != 3 || (d->order != 2 && d->order != 4 && d->order != 6) ||
+        (d->order == 6 && !d->k2_ext) || pl->p.nx < 3 || pl->p.ny < 3 || pl->p.nz < 3 || !(d->hx > 0.0) ||
+        !(d->hy > 0.0) || !(d->hz > 0.0)) {
+        set_error("hh_rhs3d: invalid arguments (a 3D plan of at least 3^3 points, order 2/4/6, f_ext, k2_ext "
+                  "for order 6, positive spacings)");
+        return HH_ERR_INVALID;
+    }
+    HH_CUDA(cudaSetDevice(pl->p.ctx->device));
+    return assemble_rhs3d(&pl->p, d, (double2 *)rhs);
 }
 
 // Host buffers: the batch goes through in chunks so that the host-to-device copy of chunk i+1,

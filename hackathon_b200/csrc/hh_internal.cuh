@@ -94,6 +94,11 @@ struct Ctx {
     // the chunk table of multi-plan solves (hh_solve_source_multi), grown on demand
     void                    *multi_tab = nullptr;
     size_t                   multi_tab_bytes = 0;
+    // the right-hand-side assembly's workspace (extended-grid derivative fields) and tables
+    double2                 *rhs_work = nullptr;
+    long                     rhs_elems = 0;
+    void                    *rhs_tab = nullptr;
+    size_t                   rhs_tab_bytes = 0;
 };
 
 int tables_for(Ctx *c, int m, const double2 **tw, const double **sn);
@@ -158,6 +163,9 @@ long slab_planes(const Plan &p, long planes); // 3D transform slab in planes (th
 // the fused-source solve of several plans of one shape in one pass (hh_solve_source_multi);
 // table: device memory of line_solve_multi_table_bytes, or nullptr for the context's own
 int solve_source_multi(Plan *const *plans, const int *nrhs, int nplans, const double2 *f, double2 *u, void *table);
+// the reference's rhs() on the device for plans of any stencil (hh_rhs2d / hh_rhs3d)
+int assemble_rhs2d(Plan *p, const hh_rhs2d_data *d, double2 *rhs);
+int assemble_rhs3d(Plan *p, const hh_rhs3d_data *d, double2 *rhs);
 int segment_count(int rows);
 int sym_default_variant(int rows);
 int padded_rows(int rows);

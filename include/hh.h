@@ -192,6 +192,45 @@ int hh_solve_source_host_noalloc(hh_plan *plan, const double *f_host, double *u_
 int hh_residual(hh_plan *plan, const double *sol_dev, const double *rhs_dev, double *res_dev, int batch,
                 double *max_res, double *max_rhs);
 
+/* The reference's right-hand-side assembly rhs() on the device, for plans of any stencil (the
+ * reference's own variable-k problems and Dirichlet data): 2D_Program/main_functions/rhs.c:4-150
+ * and 3D_Program/main_functions/rhs.c:13-194, with the compact [1 10 1] / [1 4 1] Pade derivatives
+ * of the partial_derivatives/ files solved along each axis on the device.  The data the reference
+ * evaluates through its user callbacks comes as sampled arrays, x fastest, complex unless noted;
+ * a NULL boundary array means identically zero.  rhs_dev receives nx*ny (nx*ny*nz) values, the
+ * input of hh_solve on the same plan.  The plan's stencil rows give the Dirichlet corrections.
+ * Arithmetic follows the reference's expression order (complex throughout; the reference's 3D
+ * rhs.c:149 keeps its partial sums in real doubles, which agrees for real data). */
+typedef struct {
+    int           order;        /* 2, 4 or 6                                                    */
+    double        hx, hy;       /* grid spacings                                                */
+    const double *f_ext;        /* device: f on the extended grid, (nx+2)(ny+2)                 */
+    const double *k_ext;        /* host: k at y0 + j hy, j = 0..ny+1 (order 6)                  */
+    const double *k2y_bc;       /* host: d(k^2)/dy at y0 and at y1, 2 values                    */
+    const double *fxx_xb;       /* device: f_xx on x = x0 (j = 0..ny+1), then on x = x1          */
+    const double *fxx_yb;       /* device: f_xx on y = y0 (i = 0..nx+1), then on y = y1          */
+    const double *fyy_xb;       /* device: f_yy on x = x0, then x = x1: 2 (ny+2)                */
+    const double *fyy_yb;       /* device: f_yy on y = y0, then y = y1: 2 (nx+2)                */
+    const double *fy_yb;        /* device: f_y on y = y0 at interior x (nx), then on y = y1     */
+    const double *u_xb, *u_yb;  /* device, real: Dirichlet data on x = x0, x1: 2 (ny+2); on
+                                   y = y0, y1: 2 (nx+2)                                          */
+} hh_rhs2d_data;
+int hh_rhs2d(hh_plan *plan, const hh_rhs2d_data *data, double *rhs_dev);
+
+typedef struct {
+    int           order;        /* 2, 4 or 6                                                    */
+    double        hx, hy, hz;   /* grid spacings                                                */
+    const double *f_ext;        /* device: the source on the extended grid scaled by hz^2 (the
+                                   reference's rhs_ext), (nx+2)(ny+2)(nz+2)                      */
+    const double *k2_ext;       /* host: k^2 at z0 + l hz, l = 0..nz+1 (order 6)                */
+    const double *kz_bc;        /* host: the boundary terms of d(k^2)/dz at z0 and z1, 2 values */
+    const double *fxx_b;        /* device: f_xx on x = x0 (j + l (ny+2)), then on x = x1        */
+    const double *fyy_b;        /* device: f_yy on y = y0 (i + l (nx+2)), then on y = y1        */
+    const double *fzz_b;        /* device: f_zz on z = z0 (i + j (nx+2)), then on z = z1        */
+    const double *ue_ext;       /* device: Dirichlet data on the extended grid (its z faces)    */
+} hh_rhs3d_data;
+int hh_rhs3d(hh_plan *plan, const hh_rhs3d_data *data, double *rhs_dev);
+
 /* Mixed-precision refined solve of `batch` assembled right-hand sides on the device (an
  * addition: the reference solves in plain FP64 only): every solve in
  * the loop runs its DSTs in single-precision arithmetic (where n + 1 is a power of two up to

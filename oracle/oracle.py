@@ -81,10 +81,12 @@ class Oracle:
         return out
 
     # -- 2D
-    def problem2d(self, n: int, order: int, k: complex, f_ext: np.ndarray, x0=0.0, x1=1.0, **bnd):
+    def problem2d(self, n: int, order: int, k, f_ext: np.ndarray, x0=0.0, x1=1.0, **bnd):
+        """k: a constant, or the n+2 samples k(y0 + j h) of a variable wavenumber."""
         h = (x1 - x0) / (n + 1)
         keep = {}
-        k_ext = np.full(n + 2, complex(k), dtype=np.complex128)
+        k_ext = (np.ascontiguousarray(k, dtype=np.complex128) if np.ndim(k) else
+                 np.full(n + 2, complex(k), dtype=np.complex128))
         keep["k_ext"] = k_ext
         keep["f_ext"] = np.ascontiguousarray(f_ext, dtype=np.complex128)
         pb = _Problem2D(nx=n, ny=n, order=order, x0=x0, x1=x1, y0=x0, y1=x1, hx=h, hy=h)
