@@ -86,6 +86,8 @@ SIGNATURES = {
     "hh_plan_slab": (_l, [_vp]),
     "hh_plan_set_dst_variant": (_i, [_vp, _i]),
     "hh_plan_dst_variant": (_i, [_vp]),
+    "hh_plan_set_rows_variant": (_i, [_vp, _i]),
+    "hh_plan_rows_variant": (_i, [_vp]),
     "hh_solve": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_host": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source": (_i, [_vp, _vp, _vp, _i]),
@@ -295,6 +297,15 @@ class Plan:
     @dst_variant.setter
     def dst_variant(self, v: int):
         check(lib().hh_plan_set_dst_variant(self.h, v), "hh_plan_set_dst_variant")
+
+    @property
+    def rows_variant(self) -> int:
+        """The rows-transform kernel (0: the length's default, 1: CTA ring, 2: per-warp buffers)."""
+        return int(lib().hh_plan_rows_variant(self.h))
+
+    @rows_variant.setter
+    def rows_variant(self, v: int):
+        check(lib().hh_plan_set_rows_variant(self.h, v), "hh_plan_set_rows_variant")
 
     # -- device buffers (torch tensors / raw addresses)
     def solve(self, rhs, sol, batch: int = 1):

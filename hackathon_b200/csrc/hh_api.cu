@@ -605,6 +605,35 @@ static int tune_measure(hh_plan *pl, int batch) {
     };
     rc = run();
     p.variant = best;
+    // the rows transform: the CTA ring or per-warp line buffers (lengths n + 1 = 64 .. 1024), timed
+    // as one forward and one inverse transform of the batch
+    const int mx = p.nx + 1;
+    if (rc == HH_OK && mx >= 64 && mx <= 1024 && (mx & (mx - 1)) == 0) {
+        int   best_rk = p.rows_kernel;
+        float best_t = 1e30f;
+        for (int rk = 1; rk <= 2 && rc == HH_OK; rk++) {
+            p.rows_kernel = rk;
+            auto pass = [&]() -> int {
+                HH_TRY(transform_forward(p, buf, buf, batch));
+                return transform_inverse(p, buf, batch);
+            };
+            if ((rc = pass()) != HH_OK) break;
+            if (cudaEventRecord(e0, c->stream) != cudaSuccess) { rc = HH_ERR_CUDA; break; }
+            for (int r = 0; r < 3 && rc == HH_OK; r++) rc = pass();
+            if (rc != HH_OK) break;
+            float ms = 0.f;
+            if (cudaEventRecord(e1, c->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+                rc = HH_ERR_CUDA;
+                break;
+            }
+            if (ms < best_t) {
+                best_t = ms;
+                best_rk = rk;
+            }
+        }
+        p.rows_kernel = best_rk;
+    }
     // 3D plans: the slab of the transform passes, over candidates from a sixteenth of L2 to the
     // whole batch, timed as one forward and one inverse transform
     if (rc == HH_OK && p.dim == 3) {
@@ -663,7 +692,7 @@ static int tune_measure(hh_plan *pl, int batch) {
 // mutex; hh_tune_cache_save / _load keep it in a text file (one tab-separated entry per line).
 namespace {
 struct TuneEntry {
-    int  variant = 0, col_kernel = 0;
+    int  variant = 0, col_kernel = 0, rows_kernel = 0;
     long slab = 0;
 };
 std::mutex                       g_tune_mu;
@@ -680,10 +709,11 @@ std::string tune_key(const Plan &p) {
 
 bool tune_apply(Plan &p, const TuneEntry &e) {
     if (e.variant < 0 || e.variant >= solve_variant_count() || (e.variant >= 2 && !p.sym) || e.col_kernel < 0 ||
-        e.col_kernel > 1 || e.slab < 0)
+        e.col_kernel > 1 || e.rows_kernel < 0 || e.rows_kernel > 2 || e.slab < 0)
         return false;
     p.variant = e.variant;
     p.col_kernel = e.col_kernel;
+    p.rows_kernel = e.rows_kernel;
     p.slab = e.slab;
     return true;
 }
@@ -713,6 +743,7 @@ extern "C" int hh_plan_tune(hh_plan *pl, int batch) {
     TuneEntry e;
     e.variant = pl->p.variant;
     e.col_kernel = pl->p.col_kernel;
+    e.rows_kernel = pl->p.rows_kernel;
     e.slab = pl->p.slab;
     const std::string key = tune_key(pl->p);
     std::lock_guard<std::mutex> g(g_tune_mu);
@@ -741,8 +772,11 @@ extern "C" int hh_tune_cache_save(const char *path) {
     std::lock_guard<std::mutex> g(g_tune_mu);
     FILE *f = fopen(path, "w");
     if (!f) { set_error("hh_tune_cache_save: cannot write %s", path); return HH_ERR_INVALID; }
-    fprintf(f, "# hackathon_b200 tuning cache: device, dim, nx, ny, nz, source order, kernels, variant, column kernel, slab\n");
-    for (auto &kv : g_tune) fprintf(f, "%s\t%d\t%d\t%ld\n", kv.first.c_str(), kv.second.variant, kv.second.col_kernel, kv.second.slab);
+    fprintf(f, "# hackathon_b200 tuning cache: device, dim, nx, ny, nz, source order, kernels, variant, column kernel, "
+               "slab, rows kernel\n");
+    for (auto &kv : g_tune)
+        fprintf(f, "%s\t%d\t%d\t%ld\t%d\n", kv.first.c_str(), kv.second.variant, kv.second.col_kernel, kv.second.slab,
+                kv.second.rows_kernel);
     const bool ok = fclose(f) == 0;
     if (!ok) { set_error("hh_tune_cache_save: write error on %s", path); return HH_ERR_INVALID; }
     return HH_OK;
@@ -759,13 +793,13 @@ extern "C" int hh_tune_cache_load(const char *path, long long *loaded) {
     std::lock_guard<std::mutex> g(g_tune_mu);
     while (fgets(line, sizeof line, f)) {
         if (line[0] == '#') continue;
-        // the last three tab-separated fields are the settings, the rest is the key
+        // the last four tab-separated fields are the settings, the rest is the key
         std::string l(line);
         while (!l.empty() && (l.back() == '\n' || l.back() == '\r')) l.pop_back();
-        size_t cut[3];
+        size_t cut[4];
         size_t pos = l.size();
         bool   ok = true;
-        for (int t = 0; t < 3 && ok; t++) {
+        for (int t = 0; t < 4 && ok; t++) {
             pos = l.rfind('\t', pos == 0 ? 0 : pos - 1);
             ok = pos != std::string::npos && pos > 0;
             cut[t] = pos;
@@ -773,10 +807,11 @@ extern "C" int hh_tune_cache_load(const char *path, long long *loaded) {
         if (!ok) continue;
         TuneEntry e;
         char     *end = nullptr;
-        e.variant = (int)strtol(l.c_str() + cut[2] + 1, &end, 10);
-        e.col_kernel = (int)strtol(l.c_str() + cut[1] + 1, &end, 10);
-        e.slab = strtol(l.c_str() + cut[0] + 1, &end, 10);
-        g_tune[l.substr(0, cut[2])] = e;
+        e.variant = (int)strtol(l.c_str() + cut[3] + 1, &end, 10);
+        e.col_kernel = (int)strtol(l.c_str() + cut[2] + 1, &end, 10);
+        e.slab = strtol(l.c_str() + cut[1] + 1, &end, 10);
+        e.rows_kernel = (int)strtol(l.c_str() + cut[0] + 1, &end, 10);
+        g_tune[l.substr(0, cut[3])] = e;
         n++;
     }
     fclose(f);
@@ -801,11 +836,12 @@ long hh::slab_planes(const Plan &p, long planes) {
 // lp: single-precision transform arithmetic (the refined solve's low-precision solves)
 static int transform_forward(Plan &p, const double2 *in, double2 *out, int batch, bool lp) {
     Ctx *c = p.ctx;
-    if (p.dim == 2) return launch_dst_rows(c, p.nx, (long)p.ny * batch, in, p.nx, out, p.nx, lp);
+    if (p.dim == 2) return launch_dst_rows(c, p.nx, (long)p.ny * batch, in, p.nx, out, p.nx, lp, p.rows_kernel);
     const long plane = (long)p.nx * p.ny, planes = (long)p.nz * batch, sp = slab_planes(p, planes);
     for (long p0 = 0; p0 < planes; p0 += sp) {
         const long np = std::min(sp, planes - p0);
-        HH_TRY(launch_dst_rows(c, p.nx, (long)p.ny * np, in + p0 * plane, p.nx, out + p0 * plane, p.nx, lp));
+        HH_TRY(launch_dst_rows(c, p.nx, (long)p.ny * np, in + p0 * plane, p.nx, out + p0 * plane, p.nx, lp,
+                               p.rows_kernel));
         HH_TRY(launch_dst_cols(c, p.ny, p.nx, np, out + p0 * plane, p.nx, plane, out + p0 * plane, lp, p.col_kernel));
     }
     return HH_OK;
@@ -813,12 +849,13 @@ static int transform_forward(Plan &p, const double2 *in, double2 *out, int batch
 
 static int transform_inverse(Plan &p, double2 *buf, int batch, bool lp) {
     Ctx *c = p.ctx;
-    if (p.dim == 2) return launch_dst_rows(c, p.nx, (long)p.ny * batch, buf, p.nx, buf, p.nx, lp);
+    if (p.dim == 2) return launch_dst_rows(c, p.nx, (long)p.ny * batch, buf, p.nx, buf, p.nx, lp, p.rows_kernel);
     const long plane = (long)p.nx * p.ny, planes = (long)p.nz * batch, sp = slab_planes(p, planes);
     for (long p0 = 0; p0 < planes; p0 += sp) {
         const long np = std::min(sp, planes - p0);
         HH_TRY(launch_dst_cols(c, p.ny, p.nx, np, buf + p0 * plane, p.nx, plane, buf + p0 * plane, lp, p.col_kernel));
-        HH_TRY(launch_dst_rows(c, p.nx, (long)p.ny * np, buf + p0 * plane, p.nx, buf + p0 * plane, p.nx, lp));
+        HH_TRY(launch_dst_rows(c, p.nx, (long)p.ny * np, buf + p0 * plane, p.nx, buf + p0 * plane, p.nx, lp,
+                               p.rows_kernel));
     }
     return HH_OK;
 }
@@ -844,6 +881,17 @@ extern "C" int hh_plan_set_dst_variant(hh_plan *pl, int v) {
 }
 
 extern "C" int hh_plan_dst_variant(const hh_plan *pl) { return pl ? pl->p.col_kernel : -1; }
+
+extern "C" int hh_plan_set_rows_variant(hh_plan *pl, int v) {
+    if (!pl || v < 0 || v > 2) {
+        set_error("hh_plan_set_rows_variant: invalid plan or variant (%d)", v);
+        return HH_ERR_INVALID;
+    }
+    pl->p.rows_kernel = v;
+    return HH_OK;
+}
+
+extern "C" int hh_plan_rows_variant(const hh_plan *pl) { return pl ? pl->p.rows_kernel : -1; }
 
 static int check_batch(hh_plan *pl, int batch) {
     if (!pl || batch < 0 || batch > 65535) {

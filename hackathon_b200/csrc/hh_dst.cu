@@ -1272,6 +1272,7 @@ struct DstArgs {
     const double2 *in;
     double2       *out;
     long           nlines, planes, in_ld, out_ld, in_plane, out_plane;
+    int            rows_kernel = 0; // contiguous rows of n + 1 = 64 .. 1024: 0 default, 1 CTA ring, 2 per-warp
 };
 
 template <int M, bool IS, bool OS> static int launch_fft(Ctx *c, const DstArgs &a) {
@@ -1328,9 +1329,10 @@ template <int M, bool LP> static int launch_wp(Ctx *c, const DstArgs &a) {
     return HH_OK;
 }
 
+// rows kernel: a.rows_kernel 1 = the CTA ring, 2 = per-warp buffers, 0 = the length's default
 template <int M, bool LP> static int launch_w(Ctx *c, const DstArgs &a) {
-    if constexpr (WCfg<M>::RING) return launch_wr<M, LP>(c, a);
-    else return launch_wp<M, LP>(c, a);
+    const bool ring = a.rows_kernel == 0 ? (bool)WCfg<M>::RING : a.rows_kernel == 1;
+    return ring ? launch_wr<M, LP>(c, a) : launch_wp<M, LP>(c, a);
 }
 
 // LP: single-precision arithmetic where the persistent-warp kernels serve (n + 1 = 64 .. 1024);
@@ -1385,8 +1387,9 @@ template <bool IS, bool OS, bool LP = false> static int launch_dispatch(Ctx *c, 
     return HH_OK;
 }
 
-int launch_dst_rows(Ctx *c, int n, long rows, const double2 *in, long in_ld, double2 *out, long out_ld, bool lp) {
-    DstArgs a{in, out, rows, 1, in_ld, out_ld, 0, 0};
+int launch_dst_rows(Ctx *c, int n, long rows, const double2 *in, long in_ld, double2 *out, long out_ld, bool lp,
+                    int rows_kernel) {
+    DstArgs a{in, out, rows, 1, in_ld, out_ld, 0, 0, rows_kernel};
     return lp ? launch_dispatch<false, false, true>(c, n, a) : launch_dispatch<false, false>(c, n, a);
 }
 

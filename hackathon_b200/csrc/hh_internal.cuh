@@ -124,6 +124,7 @@ struct Plan {
     int      variant = 0;        // line-solve kernel: 0/1 general (512x1, 256x2), 2..6 symmetric
     long     slab = 0;           // 3D: planes per slab of the transform passes (0: the whole batch)
     int      col_kernel = 0;     // 3D column DST: 0 CTA tiles of 8 swizzled columns, 1 per-warp tiles
+    int      rows_kernel = 0;    // rows DST (n + 1 = 64 .. 1024): 0 default, 1 CTA ring, 2 per-warp buffers
     bool     sym = false;        // const_rows and sub == super on every line (constant k)
     bool     pf_ok = false;      // order-6 partial fractions well conditioned on every line
     double2 *subt = nullptr, *diagt = nullptr; // sub/diagonal row tables (4 * rows each)
@@ -140,8 +141,10 @@ struct Plan {
 
 // lp: single-precision arithmetic (the refined solve's corrections) where the persistent-warp
 // kernels serve (n + 1 = 64 .. 1024); FP64 otherwise
+// rows_kernel (n + 1 = 64 .. 1024): 0 the length's default, 1 the CTA ring of line buffers, 2
+// per-warp line buffers
 int launch_dst_rows(Ctx *c, int n, long rows, const double2 *in, long in_ld, double2 *out, long out_ld,
-                    bool lp = false);
+                    bool lp = false, int rows_kernel = 0);
 // kern: 0 = CTA tiles of 8 swizzled columns where the length allows, 1 = per-warp tiles of LPW columns
 int launch_dst_cols(Ctx *c, int n, long ncols, long planes, const double2 *in, long ld, long plane_stride,
                     double2 *out, bool lp = false, int kern = 0);

@@ -128,7 +128,8 @@ int hh_plan_variant(const hh_plan *plan);
  * 3D_Program/solver_functions/cuda_kernels.cu:336-346).  hh_plan_tune remembers what it measured
  * per device model and problem shape (dim, nx, ny, nz, fused source order, and which line-solve
  * kernels the stencil admits; not k, which does not change which kernel is fastest) and applies
- * a remembered entry instead of timing: a cache hit launches nothing.  The cache is process-wide
+ * a remembered entry instead of timing: a cache hit launches nothing (entries: line-solve variant,
+ * column and rows transform kernels, 3D slab).  The cache is process-wide
  * and thread-safe.  hh_plan_apply_tuning applies an entry if one exists (*found = 1) and never
  * measures.  save/load keep the cache in a text file; load adds to what is cached. */
 int hh_plan_apply_tuning(hh_plan *plan, int *found);
@@ -150,6 +151,12 @@ long hh_plan_slab(const hh_plan *plan);
  * not depend on the variant. */
 int  hh_plan_set_dst_variant(hh_plan *plan, int variant);
 int  hh_plan_dst_variant(const hh_plan *plan);
+/* The kernel of the transform along x (contiguous rows) for lengths n + 1 = 64 .. 1024: 1 a CTA
+ * ring (the warps of a CTA share line buffers, the warp that frees one loads the CTA's line six
+ * tickets ahead into it), 2 per-warp double buffers, 0 (the default) the length's own choice (the
+ * ring at n + 1 = 1024).  hh_plan_tune times both for every plan.  The result does not depend on it. */
+int  hh_plan_set_rows_variant(hh_plan *plan, int variant);
+int  hh_plan_rows_variant(const hh_plan *plan);
 
 /* Solve A u = rhs for `batch` assembled right-hand sides (the reference's solver(System),
  * 2D_Program/solver_functions/solver.c:14, 3D_Program/solver_functions/solver.c:263). */

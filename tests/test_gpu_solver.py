@@ -329,3 +329,28 @@ def test_several_wavenumbers_in_one_solve(ctx, dim, n, order, variant):
         hh.solve_source_multi([plans[0], other], [1, 1], f, u)
     for p in plans:
         p.close()
+
+
+@pytest.mark.parametrize("dim,n", [(2, 255), (2, 511), (2, 1023), (2, 63), (3, 63), (3, 127)])
+def test_rows_dst_variants_give_identical_results(ctx, dim, n):
+    """The CTA-ring and the per-warp-buffer rows transforms run the same arithmetic on the same
+    values: every rows variant gives the same bits."""
+    torch = pytest.importorskip("torch")
+    g = torch.Generator().manual_seed(n + dim)
+    B = 3
+    shape = (B,) + (n,) * dim
+    f = torch.complex(torch.randn(shape, generator=g, dtype=torch.float64),
+                      torch.randn(shape, generator=g, dtype=torch.float64)).cuda()
+    plan = hh.Plan.helmholtz(ctx, dim, n, 6, 25.0)
+    outs = []
+    for v in (0, 1, 2):
+        plan.rows_variant = v
+        assert plan.rows_variant == v
+        u = torch.empty_like(f)
+        plan.solve_source(f, u, B)
+        ctx.synchronize()
+        outs.append(u.cpu())
+    assert torch.equal(outs[0], outs[1]) and torch.equal(outs[1], outs[2])
+    with pytest.raises(hh.HHError):
+        plan.rows_variant = 3
+    plan.close()

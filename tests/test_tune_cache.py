@@ -11,16 +11,16 @@ def test_cache_file_round_trip_without_a_gpu(tmp_path):
     hh.tune_cache_clear()
     src = tmp_path / "in.txt"
     src.write_text("# comment\n"
-                   "NVIDIA B200\t2\t1023\t1023\t1\t6\t2\t6\t0\t0\n"
-                   "NVIDIA B200\t3\t255\t255\t255\t6\t2\t6\t0\t1020\n"
+                   "NVIDIA B200\t2\t1023\t1023\t1\t6\t2\t6\t0\t0\t1\n"
+                   "NVIDIA B200\t3\t255\t255\t255\t6\t2\t6\t0\t1020\t2\n"
                    "garbage line without fields\n")
     assert hh.tune_cache_load(str(src)) == 2
     assert hh.tune_cache_stats()["entries"] == 2
     out = tmp_path / "out.txt"
     hh.tune_cache_save(str(out))
     lines = [x for x in out.read_text().splitlines() if not x.startswith("#")]
-    assert sorted(lines) == sorted(["NVIDIA B200\t2\t1023\t1023\t1\t6\t2\t6\t0\t0",
-                                    "NVIDIA B200\t3\t255\t255\t255\t6\t2\t6\t0\t1020"])
+    assert sorted(lines) == sorted(["NVIDIA B200\t2\t1023\t1023\t1\t6\t2\t6\t0\t0\t1",
+                                    "NVIDIA B200\t3\t255\t255\t255\t6\t2\t6\t0\t1020\t2"])
     hh.tune_cache_clear()
     assert hh.tune_cache_stats() == {"hits": 0, "misses": 0, "entries": 0}
     with pytest.raises(hh.HHError):
