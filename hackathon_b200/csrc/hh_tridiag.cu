@@ -1293,8 +1293,8 @@ static int launch_sym_t(Plan *p, const double2 *in, double2 *out, int batch, con
     return HH_OK;
 }
 
-// TIO: tile I/O where a line group is at least four lines (64-byte row pieces); narrower groups
-// keep the per-thread prefetch.
+// TIO: tile I/O where a line group is at least two lines (32-byte row pieces or wider); one-line
+// groups keep the per-thread prefetch.
 // segments per line of the symmetric kernel: a power of two P >= rows / KS with 8 <= P <= 256
 // (CW = 256 / P lines per CTA); P = 8 runs one right-hand side per pass
 static int sym_segments(int rows, int ks) {
@@ -1310,7 +1310,7 @@ static int launch_sym_src(Plan *p, const double2 *in, double2 *out, int batch, c
     case 16: return launch_sym_t<SRC, 16, MINB, NR, KS, TIO>(p, in, out, batch, multi);
     case 32: return launch_sym_t<SRC, 8, MINB, NR, KS, TIO>(p, in, out, batch, multi);
     case 64: return launch_sym_t<SRC, 4, MINB, NR, KS, TIO>(p, in, out, batch, multi);
-    case 128: return launch_sym_t<SRC, 2, MINB, NR, KS, false>(p, in, out, batch, multi);
+    case 128: return launch_sym_t<SRC, 2, MINB, NR, KS, TIO>(p, in, out, batch, multi); // 32-byte row pieces
     case 256: return launch_sym_t<SRC, 1, MINB, NR, KS, false>(p, in, out, batch, multi);
     default: set_error("symmetric line solve: %d rows", p->rows); return HH_ERR_UNSUPPORTED;
     }

@@ -116,7 +116,8 @@ long hh_plan_field_size(const hh_plan *plan);  /* complex values per right-hand 
 /* The line solve has several kernels: 0 and 1 for any stencil (512 threads x 1 block or 256 x 2
  * per SM); for constant-coefficient symmetric lines (the Helmholtz plans) also 2 (two blocks
  * per SM), 3 (one block, no register cap), 4 (two right-hand sides per pass), 5 (16-row
- * segments) and 6 (16-row segments, right-hand sides brought in as TMA tiles).  hh_plan_tune
+ * segments) and 6 (16-row segments, right-hand sides brought in as TMA tiles where a CTA holds
+ * at least two lines, i.e. lines of up to 2048 rows).  hh_plan_tune
  * times each on `batch` right-hand sides and keeps the fastest (blocking; not during stream
  * capture); set/get select one directly.  A new symmetric plan starts at 2, or at 5 for lines
  * longer than 2048 rows. */
