@@ -605,10 +605,11 @@ static int tune_measure(hh_plan *pl, int batch) {
     };
     rc = run();
     p.variant = best;
-    // the rows transform: the CTA ring or per-warp line buffers (lengths n + 1 = 64 .. 1024), timed
-    // as one forward and one inverse transform of the batch
+    // the rows transform: the CTA ring or per-warp line buffers (lengths n + 1 = 64 .. 1024), the
+    // two-warp line kernel or the Stockham kernel (2048), timed as one forward and one inverse
+    // transform of the batch
     const int mx = p.nx + 1;
-    if (rc == HH_OK && mx >= 64 && mx <= 1024 && (mx & (mx - 1)) == 0) {
+    if (rc == HH_OK && mx >= 64 && mx <= 2048 && (mx & (mx - 1)) == 0) {
         int   best_rk = p.rows_kernel;
         float best_t = 1e30f;
         for (int rk = 1; rk <= 2 && rc == HH_OK; rk++) {

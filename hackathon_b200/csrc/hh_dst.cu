@@ -938,6 +938,211 @@ __global__ void __launch_bounds__(32 * WCfg<M>::RWPC, 2)
         }
 }
 
+// ---- rows, M = 2048: two warps per line (a "team" of TL = 64 lanes, R = 32 values per lane; one
+// warp would need 64 values per lane).  With j = l + 64 q and k = k1 + 32 k2:
+//   Y_k = sum_l W_64^{l k2} [ W_M^{l k1} sum_q y_{l+64q} W_32^{q k1} ]
+// Lane l forms y_j (q < 32), runs the 32-point DFT over q and twiddles by W_M^{l k1}; a transpose
+// through the line's buffer gives each k1 (< 32) its 64 values over l.  That 64-point DFT is split
+// 64 = 2 x 32 over a lane pair of one warp (lanes w and w ^ 16 take the even and the odd l): each
+// runs a 32-point DFT and the pair finishes with one radix-2 step, exchanging half of its values
+// by shuffles.  Post-processing and the outputs are those of w_transform (KB = 16 per lane), the
+// prefix sum carried from the first warp of the team to the second through shared memory.  The
+// team synchronises on its own named barrier (64 threads).  A CTA of TPC teams shares a ring of
+// NS = TPC + 2 line buffers with the protocol of k_dst1_wr (gen[] counts the copies issued to a
+// buffer; the team that frees a buffer loads the CTA's line NS tickets ahead into it).
+template <int M> struct W2Geom;
+template <> struct W2Geom<2048> {
+    static constexpr int TL = 64, R = 32, KB = 16, TPC = 4, NS = 6;
+    static constexpr int TP = TL + 1; // transpose pitch: the 8 lanes of a phase read 8 distinct bank groups
+    // max(staged line N, transpose R * TP, Y at k + k / KB, outputs at (2KB + 1)(p / 2KB) + p % 2KB),
+    // rounded to 8 elements
+    static constexpr int BUF = (cmax(cmax(2047, R * TP), cmax(2048 + 2048 / KB, (2 * KB + 1) * (2048 / (2 * KB)))) + 7) / 8 * 8;
+    static constexpr int SMEM = 256 + 16 * NS * BUF; // barriers, counters and carries, then the buffers
+    static_assert(NS * 8 + NS * 4 <= 128 && TPC * 16 <= 128, "the header fits in 256 bytes");
+};
+
+__device__ __forceinline__ void team_sync(int id) { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
+// true on every thread of the team if p holds on any of them (a barrier of the team)
+__device__ __forceinline__ bool team_any(int id, bool p) {
+    int r;
+    asm volatile("{\n .reg .pred q, o;\n setp.ne.s32 q, %1, 0;\n bar.red.or.pred o, %2, 64, q;\n selp.s32 %0, 1, 0, o;\n}\n"
+                 : "=r"(r)
+                 : "r"((int)p), "r"(id)
+                 : "memory");
+    return r != 0;
+}
+
+template <int M>
+__global__ void __launch_bounds__(64 * W2Geom<M>::TPC, 1)
+    k_dst1_w2(const double2 *in, double2 *out, long nlines, long nplanes, long in_ld, long out_ld, long in_plane,
+              long out_plane, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
+    using G = W2Geom<M>;
+    constexpr int      TL = G::TL, R = G::R, KB = G::KB, K2 = 2 * KB, NS = G::NS, TPC = G::TPC, TP = G::TP;
+    constexpr int      N = M - 1, BUF = G::BUF;
+    constexpr uint32_t kLineBytes = N * 16;
+    extern __shared__ __align__(128) unsigned char dsm[];
+    uint64_t          *bar = reinterpret_cast<uint64_t *>(dsm);
+    volatile int      *gen = reinterpret_cast<volatile int *>(dsm + 8 * NS);
+    double2           *carry = reinterpret_cast<double2 *>(dsm + 128);
+    double2           *slots = reinterpret_cast<double2 *>(dsm + 256);
+    const int          tq = threadIdx.x >> 6, l = threadIdx.x & 63; // team, lane of the line
+    const int          h = l >> 5, w = l & 31;                       // warp of the team, lane of the warp
+    const int          k1 = 16 * h + (w & 15), e = w >> 4;           // second stage: DFT k1, even/odd l
+    const int          bid = 1 + tq;                                 // the team's named barrier
+    const long         total = nlines * nplanes;
+    if ((long)blockIdx.x >= total) return; // whole CTA
+    const int tickets = (int)((total - blockIdx.x + gridDim.x - 1) / gridDim.x);
+    auto      line_of = [&](int t) { return (long)blockIdx.x + (long)t * gridDim.x; };
+    auto      src_of = [&](long g) {
+        return nplanes == 1 ? in + g * in_ld : in + (g / nlines) * in_plane + (g % nlines) * in_ld;
+    };
+    auto dst_of = [&](long g) {
+        return nplanes == 1 ? out + g * out_ld : out + (g / nlines) * out_plane + (g % nlines) * out_ld;
+    };
+    auto fetch = [&](int t) { // one thread: ticket t into buffer t % NS
+        const int b = t % NS;
+        mbar_expect_tx(&bar[b], kLineBytes);
+        tma_bulk_load(slots + (long)b * BUF, src_of(line_of(t)), kLineBytes, &bar[b]);
+    };
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < NS; b++) {
+            mbar_init(&bar[b], 1);
+            gen[b] = 0;
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (int b = 0; b < NS && b < tickets; b++) {
+            fetch(b);
+            gen[b] = 1;
+        }
+    }
+    __syncthreads();
+    // per-lane constants: sin, cos(pi l / M); W_M^{l a} (a < 8), W_M^{8 l b} (b < R / 8)
+    double  sb = __ldg(sn + l), cb = __ldg(sn + M / 2 - l);
+    double2 twa[8], twb[R / 8];
+#pragma unroll
+    for (int a = 0; a < 8; a++) twa[a] = __ldg(tw + ((l * a) & (M - 1)));
+#pragma unroll
+    for (int b = 0; b < R / 8; b++) twb[b] = __ldg(tw + ((8 * l * b) & (M - 1)));
+    const double2 zero = make_double2(0.0, 0.0);
+    const double  coef = 0.5 * sqrt(2.0 / M);
+
+    int failed = -1;
+    for (int t = tq; t < tickets; t += TPC) {
+        const int b = t % NS;
+        const int want = t / NS + 1; // the copy of this ticket is buffer b's want-th
+        long      spin = 0;
+        while (gen[b] < want && ++spin < (1L << 26)) {
+        }
+        const bool ok = gen[b] >= want && mbar_wait_parity(&bar[b], (uint32_t)((t / NS) & 1));
+        if (team_any(bid, !ok)) {
+            if (l == 0) atomicExch(err, 1);
+            failed = t;
+            break;
+        }
+        double2 *buf = slots + (long)b * BUF;
+        // re-formed for every line (see WConst::launder): hoisted products would pin registers
+        asm volatile("" : "+d"(sb), "+d"(cb));
+#pragma unroll
+        for (int a = 0; a < 8; a++) asm volatile("" : "+d"(twa[a].x), "+d"(twa[a].y));
+#pragma unroll
+        for (int a = 0; a < R / 8; a++) asm volatile("" : "+d"(twb[a].x), "+d"(twb[a].y));
+
+        // ---- y_j = (s + 1/2) x_j + (s - 1/2) x_{M-j}, s = sin(pi j / M), j = l + TL q, at v[bitrev(q)]
+        double2 v[R];
+#pragma unroll
+        for (int q = 0; q < R; q++) {
+            const int j = l + TL * q;
+            double2   a = zero, m = zero;
+            if (q > 0 || l > 0) {
+                a = buf[j - 1];
+                m = buf[M - j - 1];
+            }
+            const double sp = fma(sb, cos_m64(q * (64 / R)), fma(cb, sin_m64(q * (64 / R)), 0.5));
+            const double sm = sp - 1.0;
+            v[bitrev_c<R>(q)] = make_double2(fma(sp, a.x, sm * m.x), fma(sp, a.y, sm * m.y));
+        }
+        team_sync(bid); // the staged line is consumed
+        dft_dit<R>(v);
+#pragma unroll
+        for (int k = 0; k < R; k++) buf[k * TP + l] = k ? cmul(v[k], cmul(twa[k & 7], twb[k >> 3])) : v[0];
+        team_sync(bid);
+
+        // ---- k1's 64-point DFT over l: this lane takes l = e + 2 m (m < 32)
+        double2 u[R];
+#pragma unroll
+        for (int m = 0; m < R; m++) u[bitrev_c<R>(m)] = buf[k1 * TP + e + 2 * m];
+        team_sync(bid); // the transposed values are consumed
+        dft_dit<R>(u);  // u[k] = A_e[k]
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            // the pair's radix-2 step: Z[k'] = A_0[k'] + W_64^{k'} A_1[k'], Z[k' + 32] = A_0[k'] - W_64^{k'} A_1[k'],
+            // this lane at k' = 16 e + i (W_64^{16 + i} = -i W_64^i)
+            const double2 own = e ? u[16 + i] : u[i];
+            const double2 snd = e ? u[i] : u[16 + i];
+            const double2 rcv = make_double2(__shfl_xor_sync(0xffffffffu, snd.x, 16), __shfl_xor_sync(0xffffffffu, snd.y, 16));
+            const double2 a0 = e ? rcv : own, a1 = e ? own : rcv;
+            double2       tt = cmul(a1, make_double2(cos_m64(2 * i), -sin_m64(2 * i)));
+            if (e) tt = make_double2(tt.y, -tt.x);
+            const int klo = k1 + 32 * (16 * e + i), khi = klo + 1024;
+            buf[klo + klo / KB] = cadd(a0, tt);
+            buf[khi + khi / KB] = csub(a0, tt);
+        }
+        team_sync(bid); // Y complete
+
+        // ---- post-processing on blocks k = KB l + u (as in w_transform)
+        double2 cs[KB], ev[KB];
+        double2 run = zero;
+#pragma unroll
+        for (int uu = 0; uu < KB; uu++) {
+            const int     k = KB * l + uu;
+            const double2 yk = buf[k + k / KB];
+            if (k == 0) {
+                cs[uu] = yk;
+                ev[uu] = zero;
+            } else {
+                const int     km = M - k;
+                const double2 ym = buf[km + km / KB];
+                cs[uu] = cadd(yk, ym);
+                ev[uu] = make_double2(ym.y - yk.y, yk.x - ym.x);
+            }
+            run = cadd(run, cs[uu]);
+            cs[uu] = run;
+        }
+        const double2 incl = line_scan<32, 1, false>(run, w);
+        if (h == 0 && w == 31) carry[tq] = incl;
+        team_sync(bid); // every read of Y is done; the first warp's total is visible
+        double2 pre = csub(incl, run);
+        if (h) pre = cadd(pre, carry[tq]);
+#pragma unroll
+        for (int uu = 0; uu < KB; uu++) {
+            const int k = KB * l + uu, po = 2 * k, pe = 2 * k - 1;
+            buf[(K2 + 1) * (po / K2) + po % K2] = cscale(cadd(pre, cs[uu]), coef);
+            if (k > 0) buf[(K2 + 1) * (pe / K2) + pe % K2] = cscale(ev[uu], coef);
+        }
+        team_sync(bid); // outputs complete
+        double2 *dst = dst_of(line_of(t));
+#pragma unroll
+        for (int q = 0; q < M / TL; q++) {
+            const int p = l + TL * q;
+            if (p < N) dst[p] = buf[(K2 + 1) * (p / K2) + p % K2];
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // reads before the refill
+        team_sync(bid);
+        if (l == 0 && t + NS < tickets) {
+            fetch(t + NS);
+            __threadfence_block(); // the copy's arrival is registered before its ticket is announced
+            gen[b] = want + 1;
+        }
+    }
+    // after an expired wait, copies issued to the ring get a bounded chance to land before the
+    // CTA's shared memory is released
+    if (failed >= 0 && l == 0)
+        for (int t = failed; t < tickets && t < failed + NS; t++) {
+            const int b = t % NS;
+            if (gen[b] >= t / NS + 1) mbar_wait_parity(&bar[b], (uint32_t)((t / NS) & 1));
+        }
+}
+
 // ---- columns: line x of plane p is element j at base + p plane + x + (j - 1) ld.  A 4-D tensor
 // map (re/im, x, j, plane) brings C = LPW neighbouring columns, all rows, into a [j][c] tile; the
 // warp's lanes interleave over the C lines (lane = c + LPW l) so that reading the tile is free of
@@ -1329,6 +1534,25 @@ template <int M, bool LP> static int launch_wp(Ctx *c, const DstArgs &a) {
     return HH_OK;
 }
 
+template <int M> static int launch_w2(Ctx *c, const DstArgs &a) {
+    using G = W2Geom<M>;
+    const double2 *tw;
+    const double  *sn;
+    HH_TRY(tables_for(c, M, &tw, &sn));
+    HH_CUDA(cudaFuncSetAttribute(k_dst1_w2<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
+    int dev = 0, sms = 148, per_sm = 0;
+    HH_CUDA(cudaGetDevice(&dev));
+    HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dst1_w2<M>, 64 * G::TPC, G::SMEM));
+    const long lines = a.nlines * a.planes;
+    const long ctas = std::min<long>((lines + G::TPC - 1) / G::TPC, (long)std::max(1, per_sm) * sms);
+    k_dst1_w2<M><<<(unsigned)ctas, 64 * G::TPC, G::SMEM, c->stream>>>(a.in, a.out, a.nlines, a.planes, a.in_ld, a.out_ld,
+                                                                    a.in_plane, a.out_plane, tw, sn, c->err_word);
+    HH_CUDA(cudaGetLastError());
+    c->launches++;
+    return HH_OK;
+}
+
 // rows kernel: a.rows_kernel 1 = the CTA ring, 2 = per-warp buffers, 0 = the length's default
 template <int M, bool LP> static int launch_w(Ctx *c, const DstArgs &a) {
     const bool ring = a.rows_kernel == 0 ? (bool)WCfg<M>::RING : a.rows_kernel == 1;
@@ -1352,6 +1576,9 @@ template <bool IS, bool OS, bool LP = false> static int launch_dispatch(Ctx *c, 
         case 256: return launch_w<256, LP>(c, a);
         case 512: return launch_w<512, LP>(c, a);
         case 1024: return launch_w<1024, LP>(c, a);
+        case 2048: // two warps per line (FP64 only); rows_kernel 2 keeps the Stockham kernel below
+            if (!LP && a.rows_kernel != 2) return launch_w2<2048>(c, a);
+            break;
         default: break;
         }
     }

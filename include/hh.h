@@ -155,7 +155,9 @@ int  hh_plan_dst_variant(const hh_plan *plan);
 /* The kernel of the transform along x (contiguous rows) for lengths n + 1 = 64 .. 1024: 1 a CTA
  * ring (the warps of a CTA share line buffers, the warp that frees one loads the CTA's line six
  * tickets ahead into it), 2 per-warp double buffers, 0 (the default) the length's own choice (the
- * ring at n + 1 = 1024).  hh_plan_tune times both for every plan.  The result does not depend on it. */
+ * ring at n + 1 = 1024).  The result does not depend on it.  At n + 1 = 2048: 0 and 1 two warps
+ * per line (in a CTA ring), 2 the Stockham kernel of the longer lengths; the two agree to
+ * rounding.  hh_plan_tune times both choices for every plan of these lengths. */
 int  hh_plan_set_rows_variant(hh_plan *plan, int variant);
 int  hh_plan_rows_variant(const hh_plan *plan);
 

@@ -47,6 +47,23 @@ def test_dst_rows_1023_ring_ticket_counts(ctx, oracle, rows):
     assert rel_err(_host(dst), oracle.dst1_rows(x)) < 1e-13
 
 
+@pytest.mark.parametrize("rows", [1, 3, 593, 888, 889, 3001])
+def test_dst_rows_2047_two_warp_ticket_counts(ctx, oracle, rows):
+    """2047-point rows go through the two-warps-per-line kernel (four lines per block, six line
+    buffers, one block per SM): fewer lines than teams, one more line than the 592 teams of 148
+    blocks, exactly the 888 buffers, one more, and thousands of rows spread unevenly."""
+    n = 2047
+    rng = np.random.default_rng(rows + 7)
+    x = rng.standard_normal((rows, n)) + 1j * rng.standard_normal((rows, n))
+    src, dst = _dev(x), torch.empty((rows, n), dtype=torch.complex128, device="cuda")
+    ctx.dst1_rows(n, rows, src, dst)
+    ctx.synchronize()
+    assert rel_err(_host(dst), oracle.dst1_rows(x)) < 1e-13
+    ctx.dst1_rows(n, rows, dst, dst)  # in place, and the transform is its own inverse
+    ctx.synchronize()
+    assert rel_err(_host(dst), x) < 1e-13
+
+
 def test_dst_rows_golden_and_in_place(ctx):
     g = golden("dst_rows.npz")
     for n in (1, 7, 31, 63, 100):

@@ -354,3 +354,26 @@ def test_rows_dst_variants_give_identical_results(ctx, dim, n):
     with pytest.raises(hh.HHError):
         plan.rows_variant = 3
     plan.close()
+
+
+def test_rows_2047_two_warp_and_stockham_kernels_agree(ctx):
+    """At n + 1 = 2048 the rows variants 0 and 1 run the two-warps-per-line transform and variant 2
+    the first-design Stockham kernel: different arithmetic, so the solutions agree to rounding
+    as the solve amplifies it (relative 1e-12, the solution parity bound; 2e-13 measured at
+    k = 100), and 0 and 1 give the same bits."""
+    torch = pytest.importorskip("torch")
+    g = torch.Generator().manual_seed(2047)
+    n, B = 2047, 2
+    f = torch.complex(torch.randn((B, n, n), generator=g, dtype=torch.float64),
+                      torch.randn((B, n, n), generator=g, dtype=torch.float64)).cuda()
+    plan = hh.Plan.helmholtz(ctx, 2, n, 6, 100.0)
+    outs = []
+    for v in (0, 1, 2):
+        plan.rows_variant = v
+        u = torch.empty_like(f)
+        plan.solve_source(f, u, B)
+        ctx.synchronize()
+        outs.append(u.cpu())
+    assert torch.equal(outs[0], outs[1])
+    assert ((outs[2] - outs[0]).abs().max() / outs[0].abs().max()).item() < 1e-12
+    plan.close()
