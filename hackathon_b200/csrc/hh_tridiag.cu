@@ -624,7 +624,7 @@ template <int NW, int CW, int NR> struct SymSmem {
     double2 AwF[NW][CW], AwB[NW][CW]; // warp totals of the segment multipliers (main solve)
     double  awF[NW][CW], awB[NW][CW]; // the same for the Pade solve (real multipliers)
     double2 BwF[NR][NW][CW], BwB[NR][NW][CW]; // warp totals of the B values, per right-hand side
-    double2 EF[NR][NW][CW], EB[NR][NW][CW];   // value entering each warp
+    double2 EF[NR][NW][CW], EB[NR][NW][CW];   // value entering each warp (order 6)
     double2 bwF[NR][NW][CW], bwB[NR][NW][CW];
     double2 eF[NR][NW][CW], eB[NR][NW][CW];
     double  pl[9], pu[9];
@@ -717,8 +717,10 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
     constexpr int SLOTS = KS + 2;
     constexpr int  NBUF = SymTileBufs<SRC>::value;
     static_assert(!TIO || NR == 1, "tile I/O moves one right-hand side at a time");
-    // cross-warp sequential passes: main solve on threads [0, CW NR), Pade solve on [128, 128 + CW NR)
-    static_assert(CW * NR <= 128 && NT >= 256, "cross-warp thread ranges");
+    // order 6: the warps' entering values are composed in sequence (threads [0, CW NR) for the
+    // main solve, [128, 128 + CW NR) for the Pade solve)
+    constexpr bool SEQ = SRC == 6;
+    static_assert(!SEQ || (CW * NR <= 128 && NT >= 256), "cross-warp thread ranges");
     const int     t = threadIdx.x;
     const double2 zero = make_double2(0.0, 0.0);
     // Orders 0-4 keep the forward multipliers L_k and the reciprocal pivots ui_k in registers.
@@ -873,32 +875,51 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
         } else {
             __syncthreads();
         }
-        if (t < CW * NR) {
-            const int r = t / CW, cc = t % CW;
-            double2   E = zero;
+        // The value entering each warp's segments of line c: the totals of the warps before it,
+        // composed in order.  Orders 0-4: every warp forms its own (the totals stay until the next
+        // barrier).  Order 6, whose two solves leave no registers for that: CW threads per solve
+        // compose them in sequence into shared memory, behind one more barrier.
+        if constexpr (SEQ) {
+            if (t < CW * NR) {
+                const int r = t / CW, cc = t % CW;
+                double2   E = zero;
 #pragma unroll
-            for (int x = 0; x < NW; x++) {
-                sm.EF[r][x][cc] = E;
-                E = zfma(sm.BwF[r][x][cc], sm.AwF[x][cc], E);
-            }
-        } else if (SRC == 6 && t >= 128 && t < 128 + CW * NR) {
-            const int r = (t - 128) / CW, cc = (t - 128) % CW;
-            double2   E = zero;
+                for (int x = 0; x < NW; x++) {
+                    sm.EF[r][x][cc] = E;
+                    E = zfma(sm.BwF[r][x][cc], sm.AwF[x][cc], E);
+                }
+            } else if (t >= 128 && t < 128 + CW * NR) {
+                const int r = (t - 128) / CW, cc = (t - 128) % CW;
+                double2   E = zero;
 #pragma unroll
-            for (int x = 0; x < NW; x++) {
-                sm.eF[r][x][cc] = E;
-                E = zaxpy(sm.bwF[r][x][cc], sm.awF[x][cc], E);
+                for (int x = 0; x < NW; x++) {
+                    sm.eF[r][x][cc] = E;
+                    E = zaxpy(sm.bwF[r][x][cc], sm.awF[x][cc], E);
+                }
             }
+            __syncthreads();
         }
-        __syncthreads();
         {
+            double2 EF[NR];
+#pragma unroll
+            for (int r = 0; r < NR; r++) EF[r] = zero;
+            if constexpr (!SEQ) {
+#pragma unroll
+                for (int x = 0; x < NW - 1; x++) {
+                    if (x < w) {
+                        const double2 a = lds_keep(&sm.AwF[x][c]);
+#pragma unroll
+                        for (int r = 0; r < NR; r++) EF[r] = zfma(sm.BwF[r][x][c], a, EF[r]);
+                    }
+                }
+            }
             const double2 AeF = lds_keep(tabF + LOG * NT + t);
             double        aeF = 0.0;
             if constexpr (SRC == 6) aeF = lds_keep(ttF + LOG * NT + t);
             double2 y[NR], z[NR];
 #pragma unroll
             for (int r = 0; r < NR; r++) {
-                y[r] = zfma(Bfe[r], AeF, sm.EF[r][w][c]);
+                y[r] = zfma(Bfe[r], AeF, SEQ ? sm.EF[r][w][c] : EF[r]);
                 z[r] = zero;
                 if constexpr (SRC == 6) z[r] = zaxpy(bfe[r], aeF, sm.eF[r][w][c]);
             }
@@ -956,32 +977,49 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
             if (sl == SPW - 1) { Bbe[r] = zero; bbe[r] = zero; }
         }
         __syncthreads();
-        if (t < CW * NR) {
-            const int r = t / CW, cc = t % CW;
-            double2   E = zero;
+        // the value entering each warp from the warps after it, composed from the last one down
+        // (as in the forward direction)
+        if constexpr (SEQ) {
+            if (t < CW * NR) {
+                const int r = t / CW, cc = t % CW;
+                double2   E = zero;
 #pragma unroll
-            for (int x = NW - 1; x >= 0; x--) {
-                sm.EB[r][x][cc] = E;
-                E = zfma(sm.BwB[r][x][cc], sm.AwB[x][cc], E);
-            }
-        } else if (SRC == 6 && t >= 128 && t < 128 + CW * NR) {
-            const int r = (t - 128) / CW, cc = (t - 128) % CW;
-            double2   E = zero;
+                for (int x = NW - 1; x >= 0; x--) {
+                    sm.EB[r][x][cc] = E;
+                    E = zfma(sm.BwB[r][x][cc], sm.AwB[x][cc], E);
+                }
+            } else if (t >= 128 && t < 128 + CW * NR) {
+                const int r = (t - 128) / CW, cc = (t - 128) % CW;
+                double2   E = zero;
 #pragma unroll
-            for (int x = NW - 1; x >= 0; x--) {
-                sm.eB[r][x][cc] = E;
-                E = zaxpy(sm.bwB[r][x][cc], sm.awB[x][cc], E);
+                for (int x = NW - 1; x >= 0; x--) {
+                    sm.eB[r][x][cc] = E;
+                    E = zaxpy(sm.bwB[r][x][cc], sm.awB[x][cc], E);
+                }
             }
+            __syncthreads();
         }
-        __syncthreads();
         {
+            double2 EB[NR];
+#pragma unroll
+            for (int r = 0; r < NR; r++) EB[r] = zero;
+            if constexpr (!SEQ) {
+#pragma unroll
+                for (int xw = NW - 1; xw > 0; xw--) {
+                    if (xw > w) {
+                        const double2 a = lds_keep(&sm.AwB[xw][c]);
+#pragma unroll
+                        for (int r = 0; r < NR; r++) EB[r] = zfma(sm.BwB[r][xw][c], a, EB[r]);
+                    }
+                }
+            }
             const double2 AeB = lds_keep(tabB + LOG * NT + t);
             double        aeB = 0.0;
             if constexpr (SRC == 6) aeB = lds_keep(ttB + LOG * NT + t);
             double2 x[NR], ww[NR];
 #pragma unroll
             for (int r = 0; r < NR; r++) {
-                x[r] = zfma(Bbe[r], AeB, sm.EB[r][w][c]);
+                x[r] = zfma(Bbe[r], AeB, SEQ ? sm.EB[r][w][c] : EB[r]);
                 ww[r] = zero;
                 if constexpr (SRC == 6) ww[r] = zaxpy(bbe[r], aeB, sm.eB[r][w][c]);
             }
