@@ -414,23 +414,28 @@ def dst_gemm_probe(torch, st, n: int = N, batch: int = BATCH) -> dict:
     """The DST of the headline step as a dense tensor-core product, measured: the orthonormal
     DST-I of batch x n complex rows is the real product [2 batch n, n] x [n, n] with the sine
     matrix; in BF16x3 (each operand split into bf16 high and low parts, hi*hi + hi*lo + lo*hi
-    with FP32 accumulation) that is three bf16 GEMMs.  cuBLAS (torch.matmul) stands in for the
+    with FP32 accumulation and FP32 outputs) that is three bf16 GEMMs.  cuBLAS (torch.mm) stands in for the
     best tensor-core kernel: its time is a lower bound for a hand-written one.  Compared with the
     FP64 FFT-based DST of the step (the `dst_forward` stage), on time and on accuracy against
     FP64 for one row block."""
+    # K and N padded to a multiple of 64 with zeros (aligned tensor-core tiles); FP32 outputs
+    npad = (n + 63) // 64 * 64
     j = torch.arange(1, n + 1, dtype=torch.float64, device="cuda")
-    S = torch.sin(math.pi * torch.outer(j, j) / (n + 1)) * math.sqrt(2.0 / (n + 1))
+    S = torch.zeros((npad, npad), dtype=torch.float64, device="cuda")
+    S[:n, :n] = torch.sin(math.pi * torch.outer(j, j) / (n + 1)) * math.sqrt(2.0 / (n + 1))
     g = torch.Generator(device="cuda").manual_seed(7)
-    X = torch.randn((2 * batch * n, n), dtype=torch.float64, device="cuda", generator=g)
+    X = torch.zeros((2 * batch * n, npad), dtype=torch.float64, device="cuda")
+    X[:, :n] = torch.randn((2 * batch * n, n), dtype=torch.float64, device="cuda", generator=g)
     s_hi = S.to(torch.bfloat16)
     s_lo = (S - s_hi.double()).to(torch.bfloat16)
     x_hi = X.to(torch.bfloat16)
     x_lo = (X - x_hi.double()).to(torch.bfloat16)
+    f32 = torch.float32
 
     def gemms():
-        torch.matmul(x_hi, s_hi)
-        torch.matmul(x_hi, s_lo)
-        torch.matmul(x_lo, s_hi)
+        torch.mm(x_hi, s_hi, out_dtype=f32)
+        torch.mm(x_hi, s_lo, out_dtype=f32)
+        torch.mm(x_lo, s_hi, out_dtype=f32)
 
     with torch.cuda.stream(st):
         for _ in range(3):
@@ -446,13 +451,13 @@ def dst_gemm_probe(torch, st, n: int = N, batch: int = BATCH) -> dict:
         ms = e0.elapsed_time(e1) / reps
         rows = 4096
         ref = X[:rows] @ S
-        approx = (torch.matmul(x_hi[:rows], s_hi).double() + torch.matmul(x_hi[:rows], s_lo).double() +
-                  torch.matmul(x_lo[:rows], s_hi).double())
+        approx = (torch.mm(x_hi[:rows], s_hi, out_dtype=f32).double() + torch.mm(x_hi[:rows], s_lo, out_dtype=f32).double() +
+                  torch.mm(x_lo[:rows], s_hi, out_dtype=f32).double())
         err = float((approx - ref).abs().max() / ref.abs().max())
-    flops = 3 * 2.0 * (2 * batch * n) * n * n
+    flops = 3 * 2.0 * (2 * batch * n) * npad * npad
     del X, x_hi, x_lo
     torch.cuda.empty_cache()
-    return {"shape": f"3 x bf16 GEMM [{2 * batch * n} x {n}] x [{n} x {n}] (cuBLAS)", "ms_per_step_dst": ms,
+    return {"shape": f"3 x bf16 GEMM [{2 * batch * n} x {npad}] x [{npad} x {npad}], FP32 out (cuBLAS)", "ms_per_step_dst": ms,
             "tflops": flops / (ms / 1000.0) / 1e12, "rel_err_vs_fp64": err,
             "note": "one forward DST of the 64-RHS step; compare stage_ms_per_solve_batch.dst_forward (FP64 FFT)"}
 
