@@ -972,7 +972,101 @@ __device__ __forceinline__ bool team_any(int id, bool p) {
     return r != 0;
 }
 
+// One line of the two-warp transform in single-precision arithmetic (the refined solve's correction
+// transforms): the staged line x_1..x_N at buf[0..N-1] in, the outputs at
+// buf[(2KB + 1)(p / 2KB) + p % 2KB] out, FP64 in and out with float exchanges in the same buffer
+// (as w_transform_lp does for one warp per line).  l: lane of the line; h, w: warp of the team and
+// lane of the warp; (k1, e): the lane's second-stage DFT and half; tq, bid: the team and its named
+// barrier; carry: the team's slot for the prefix sum.  The FP64 form is written out in k_dst1_w2.
 template <int M>
+__device__ __forceinline__ void w2_transform_lp(double2 *buf, int l, int h, int w, int k1, int e, int tq, int bid,
+                                                double sbd, double cbd, const double2 (&twad)[8],
+                                                const double2 (&twbd)[W2Geom<M>::R / 8], double2 *carry) {
+    using G = W2Geom<M>;
+    constexpr int TL = G::TL, R = G::R, KB = G::KB, K2 = 2 * KB, TP = G::TP;
+    const float2  zero = make_float2(0.f, 0.f);
+    float2       *fb = reinterpret_cast<float2 *>(buf);
+    float2       *fcarry = reinterpret_cast<float2 *>(carry);
+    const float   sb = (float)sbd, cb = (float)cbd;
+    float2        twa[8], twb[R / 8];
+#pragma unroll
+    for (int a = 0; a < 8; a++) twa[a] = make_float2((float)twad[a].x, (float)twad[a].y);
+#pragma unroll
+    for (int a = 0; a < R / 8; a++) twb[a] = make_float2((float)twbd[a].x, (float)twbd[a].y);
+
+    float2 v[R];
+#pragma unroll
+    for (int q = 0; q < R; q++) {
+        const int j = l + TL * q;
+        double2   a = make_double2(0.0, 0.0), m = a;
+        if (q > 0 || l > 0) {
+            a = buf[j - 1];
+            m = buf[M - j - 1];
+        }
+        const float sp = fmaf(sb, (float)cos_m64(q * (64 / R)), fmaf(cb, (float)sin_m64(q * (64 / R)), 0.5f));
+        const float sm = sp - 1.0f;
+        v[bitrev_c<R>(q)] = make_float2(fmaf(sp, (float)a.x, sm * (float)m.x), fmaf(sp, (float)a.y, sm * (float)m.y));
+    }
+    team_sync(bid); // the staged line is consumed
+    dft_dit_f<R>(v);
+#pragma unroll
+    for (int k = 0; k < R; k++) fb[k * TP + l] = k ? fmul2(v[k], fmul2(twa[k & 7], twb[k >> 3])) : v[0];
+    team_sync(bid);
+
+    float2 u[R];
+#pragma unroll
+    for (int m = 0; m < R; m++) u[bitrev_c<R>(m)] = fb[k1 * TP + e + 2 * m];
+    team_sync(bid);
+    dft_dit_f<R>(u);
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        const float2 own = e ? u[16 + i] : u[i];
+        const float2 snd = e ? u[i] : u[16 + i];
+        const float2 rcv = make_float2(__shfl_xor_sync(0xffffffffu, snd.x, 16), __shfl_xor_sync(0xffffffffu, snd.y, 16));
+        const float2 a0 = e ? rcv : own, a1 = e ? own : rcv;
+        float2       tt = fmul2(a1, make_float2((float)cos_m64(2 * i), -(float)sin_m64(2 * i)));
+        if (e) tt = make_float2(tt.y, -tt.x);
+        const int klo = k1 + 32 * (16 * e + i), khi = klo + 1024;
+        fb[klo + klo / KB] = fadd2(a0, tt);
+        fb[khi + khi / KB] = fsub2(a0, tt);
+    }
+    team_sync(bid);
+
+    float2 cs[KB], ev[KB];
+    float2 run = zero;
+#pragma unroll
+    for (int uu = 0; uu < KB; uu++) {
+        const int    k = KB * l + uu;
+        const float2 yk = fb[k + k / KB];
+        if (k == 0) {
+            cs[uu] = yk;
+            ev[uu] = zero;
+        } else {
+            const int    km = M - k;
+            const float2 ym = fb[km + km / KB];
+            cs[uu] = fadd2(yk, ym);
+            ev[uu] = make_float2(ym.y - yk.y, yk.x - ym.x);
+        }
+        run = fadd2(run, cs[uu]);
+        cs[uu] = run;
+    }
+    const float2 incl = line_scan_f<32, 1, false>(run, w);
+    if (h == 0 && w == 31) fcarry[2 * tq] = incl;
+    team_sync(bid);
+    float2 pre = fsub2(incl, run);
+    if (h) pre = fadd2(pre, fcarry[2 * tq]);
+    const float coef = (float)(0.5 * sqrt(2.0 / M));
+#pragma unroll
+    for (int uu = 0; uu < KB; uu++) {
+        const int    k = KB * l + uu, po = 2 * k, pe = 2 * k - 1;
+        const float2 o = fadd2(pre, cs[uu]);
+        buf[(K2 + 1) * (po / K2) + po % K2] = make_double2((double)(o.x * coef), (double)(o.y * coef));
+        if (k > 0) buf[(K2 + 1) * (pe / K2) + pe % K2] = make_double2((double)(ev[uu].x * coef), (double)(ev[uu].y * coef));
+    }
+    team_sync(bid); // outputs complete
+}
+
+template <int M, bool LP = false>
 __global__ void __launch_bounds__(64 * W2Geom<M>::TPC, 1)
     k_dst1_w2(const double2 *in, double2 *out, long nlines, long nplanes, long in_ld, long out_ld, long in_plane,
               long out_plane, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
@@ -1047,79 +1141,83 @@ __global__ void __launch_bounds__(64 * W2Geom<M>::TPC, 1)
 #pragma unroll
         for (int a = 0; a < R / 8; a++) asm volatile("" : "+d"(twb[a].x), "+d"(twb[a].y));
 
-        // ---- y_j = (s + 1/2) x_j + (s - 1/2) x_{M-j}, s = sin(pi j / M), j = l + TL q, at v[bitrev(q)]
-        double2 v[R];
-#pragma unroll
-        for (int q = 0; q < R; q++) {
-            const int j = l + TL * q;
-            double2   a = zero, m = zero;
-            if (q > 0 || l > 0) {
-                a = buf[j - 1];
-                m = buf[M - j - 1];
+        if constexpr (LP) {
+            w2_transform_lp<M>(buf, l, h, w, k1, e, tq, bid, sb, cb, twa, twb, carry);
+        } else {
+            // ---- y_j = (s + 1/2) x_j + (s - 1/2) x_{M-j}, s = sin(pi j / M), j = l + TL q, at v[bitrev(q)]
+            double2 v[R];
+    #pragma unroll
+            for (int q = 0; q < R; q++) {
+                const int j = l + TL * q;
+                double2   a = zero, m = zero;
+                if (q > 0 || l > 0) {
+                    a = buf[j - 1];
+                    m = buf[M - j - 1];
+                }
+                const double sp = fma(sb, cos_m64(q * (64 / R)), fma(cb, sin_m64(q * (64 / R)), 0.5));
+                const double sm = sp - 1.0;
+                v[bitrev_c<R>(q)] = make_double2(fma(sp, a.x, sm * m.x), fma(sp, a.y, sm * m.y));
             }
-            const double sp = fma(sb, cos_m64(q * (64 / R)), fma(cb, sin_m64(q * (64 / R)), 0.5));
-            const double sm = sp - 1.0;
-            v[bitrev_c<R>(q)] = make_double2(fma(sp, a.x, sm * m.x), fma(sp, a.y, sm * m.y));
-        }
-        team_sync(bid); // the staged line is consumed
-        dft_dit<R>(v);
-#pragma unroll
-        for (int k = 0; k < R; k++) buf[k * TP + l] = k ? cmul(v[k], cmul(twa[k & 7], twb[k >> 3])) : v[0];
-        team_sync(bid);
+            team_sync(bid); // the staged line is consumed
+            dft_dit<R>(v);
+    #pragma unroll
+            for (int k = 0; k < R; k++) buf[k * TP + l] = k ? cmul(v[k], cmul(twa[k & 7], twb[k >> 3])) : v[0];
+            team_sync(bid);
 
-        // ---- k1's 64-point DFT over l: this lane takes l = e + 2 m (m < 32)
-        double2 u[R];
-#pragma unroll
-        for (int m = 0; m < R; m++) u[bitrev_c<R>(m)] = buf[k1 * TP + e + 2 * m];
-        team_sync(bid); // the transposed values are consumed
-        dft_dit<R>(u);  // u[k] = A_e[k]
-#pragma unroll
-        for (int i = 0; i < 16; i++) {
-            // the pair's radix-2 step: Z[k'] = A_0[k'] + W_64^{k'} A_1[k'], Z[k' + 32] = A_0[k'] - W_64^{k'} A_1[k'],
-            // this lane at k' = 16 e + i (W_64^{16 + i} = -i W_64^i)
-            const double2 own = e ? u[16 + i] : u[i];
-            const double2 snd = e ? u[i] : u[16 + i];
-            const double2 rcv = make_double2(__shfl_xor_sync(0xffffffffu, snd.x, 16), __shfl_xor_sync(0xffffffffu, snd.y, 16));
-            const double2 a0 = e ? rcv : own, a1 = e ? own : rcv;
-            double2       tt = cmul(a1, make_double2(cos_m64(2 * i), -sin_m64(2 * i)));
-            if (e) tt = make_double2(tt.y, -tt.x);
-            const int klo = k1 + 32 * (16 * e + i), khi = klo + 1024;
-            buf[klo + klo / KB] = cadd(a0, tt);
-            buf[khi + khi / KB] = csub(a0, tt);
-        }
-        team_sync(bid); // Y complete
-
-        // ---- post-processing on blocks k = KB l + u (as in w_transform)
-        double2 cs[KB], ev[KB];
-        double2 run = zero;
-#pragma unroll
-        for (int uu = 0; uu < KB; uu++) {
-            const int     k = KB * l + uu;
-            const double2 yk = buf[k + k / KB];
-            if (k == 0) {
-                cs[uu] = yk;
-                ev[uu] = zero;
-            } else {
-                const int     km = M - k;
-                const double2 ym = buf[km + km / KB];
-                cs[uu] = cadd(yk, ym);
-                ev[uu] = make_double2(ym.y - yk.y, yk.x - ym.x);
+            // ---- k1's 64-point DFT over l: this lane takes l = e + 2 m (m < 32)
+            double2 u[R];
+    #pragma unroll
+            for (int m = 0; m < R; m++) u[bitrev_c<R>(m)] = buf[k1 * TP + e + 2 * m];
+            team_sync(bid); // the transposed values are consumed
+            dft_dit<R>(u);  // u[k] = A_e[k]
+    #pragma unroll
+            for (int i = 0; i < 16; i++) {
+                // the pair's radix-2 step: Z[k'] = A_0[k'] + W_64^{k'} A_1[k'], Z[k' + 32] = A_0[k'] - W_64^{k'} A_1[k'],
+                // this lane at k' = 16 e + i (W_64^{16 + i} = -i W_64^i)
+                const double2 own = e ? u[16 + i] : u[i];
+                const double2 snd = e ? u[i] : u[16 + i];
+                const double2 rcv = make_double2(__shfl_xor_sync(0xffffffffu, snd.x, 16), __shfl_xor_sync(0xffffffffu, snd.y, 16));
+                const double2 a0 = e ? rcv : own, a1 = e ? own : rcv;
+                double2       tt = cmul(a1, make_double2(cos_m64(2 * i), -sin_m64(2 * i)));
+                if (e) tt = make_double2(tt.y, -tt.x);
+                const int klo = k1 + 32 * (16 * e + i), khi = klo + 1024;
+                buf[klo + klo / KB] = cadd(a0, tt);
+                buf[khi + khi / KB] = csub(a0, tt);
             }
-            run = cadd(run, cs[uu]);
-            cs[uu] = run;
+            team_sync(bid); // Y complete
+
+            // ---- post-processing on blocks k = KB l + u (as in w_transform)
+            double2 cs[KB], ev[KB];
+            double2 run = zero;
+    #pragma unroll
+            for (int uu = 0; uu < KB; uu++) {
+                const int     k = KB * l + uu;
+                const double2 yk = buf[k + k / KB];
+                if (k == 0) {
+                    cs[uu] = yk;
+                    ev[uu] = zero;
+                } else {
+                    const int     km = M - k;
+                    const double2 ym = buf[km + km / KB];
+                    cs[uu] = cadd(yk, ym);
+                    ev[uu] = make_double2(ym.y - yk.y, yk.x - ym.x);
+                }
+                run = cadd(run, cs[uu]);
+                cs[uu] = run;
+            }
+            const double2 incl = line_scan<32, 1, false>(run, w);
+            if (h == 0 && w == 31) carry[tq] = incl;
+            team_sync(bid); // every read of Y is done; the first warp's total is visible
+            double2 pre = csub(incl, run);
+            if (h) pre = cadd(pre, carry[tq]);
+    #pragma unroll
+            for (int uu = 0; uu < KB; uu++) {
+                const int k = KB * l + uu, po = 2 * k, pe = 2 * k - 1;
+                buf[(K2 + 1) * (po / K2) + po % K2] = cscale(cadd(pre, cs[uu]), coef);
+                if (k > 0) buf[(K2 + 1) * (pe / K2) + pe % K2] = cscale(ev[uu], coef);
+            }
+            team_sync(bid); // outputs complete
         }
-        const double2 incl = line_scan<32, 1, false>(run, w);
-        if (h == 0 && w == 31) carry[tq] = incl;
-        team_sync(bid); // every read of Y is done; the first warp's total is visible
-        double2 pre = csub(incl, run);
-        if (h) pre = cadd(pre, carry[tq]);
-#pragma unroll
-        for (int uu = 0; uu < KB; uu++) {
-            const int k = KB * l + uu, po = 2 * k, pe = 2 * k - 1;
-            buf[(K2 + 1) * (po / K2) + po % K2] = cscale(cadd(pre, cs[uu]), coef);
-            if (k > 0) buf[(K2 + 1) * (pe / K2) + pe % K2] = cscale(ev[uu], coef);
-        }
-        team_sync(bid); // outputs complete
         double2 *dst = dst_of(line_of(t));
 #pragma unroll
         for (int q = 0; q < M / TL; q++) {
@@ -1477,7 +1575,7 @@ struct DstArgs {
     const double2 *in;
     double2       *out;
     long           nlines, planes, in_ld, out_ld, in_plane, out_plane;
-    int            rows_kernel = 0; // contiguous rows of n + 1 = 64 .. 1024: 0 default, 1 CTA ring, 2 per-warp
+    int            rows_kernel = 0; // contiguous rows: 0 default, 1 CTA ring, 2 per-warp (2048: the Stockham kernel)
 };
 
 template <int M, bool IS, bool OS> static int launch_fft(Ctx *c, const DstArgs &a) {
@@ -1534,20 +1632,21 @@ template <int M, bool LP> static int launch_wp(Ctx *c, const DstArgs &a) {
     return HH_OK;
 }
 
-template <int M> static int launch_w2(Ctx *c, const DstArgs &a) {
+template <int M, bool LP> static int launch_w2(Ctx *c, const DstArgs &a) {
     using G = W2Geom<M>;
     const double2 *tw;
     const double  *sn;
     HH_TRY(tables_for(c, M, &tw, &sn));
-    HH_CUDA(cudaFuncSetAttribute(k_dst1_w2<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
+    HH_CUDA(cudaFuncSetAttribute(k_dst1_w2<M, LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
     int dev = 0, sms = 148, per_sm = 0;
     HH_CUDA(cudaGetDevice(&dev));
     HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dst1_w2<M>, 64 * G::TPC, G::SMEM));
+    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dst1_w2<M, LP>, 64 * G::TPC, G::SMEM));
     const long lines = a.nlines * a.planes;
     const long ctas = std::min<long>((lines + G::TPC - 1) / G::TPC, (long)std::max(1, per_sm) * sms);
-    k_dst1_w2<M><<<(unsigned)ctas, 64 * G::TPC, G::SMEM, c->stream>>>(a.in, a.out, a.nlines, a.planes, a.in_ld, a.out_ld,
-                                                                    a.in_plane, a.out_plane, tw, sn, c->err_word);
+    k_dst1_w2<M, LP><<<(unsigned)ctas, 64 * G::TPC, G::SMEM, c->stream>>>(a.in, a.out, a.nlines, a.planes, a.in_ld,
+                                                                        a.out_ld, a.in_plane, a.out_plane, tw, sn,
+                                                                        c->err_word);
     HH_CUDA(cudaGetLastError());
     c->launches++;
     return HH_OK;
@@ -1559,7 +1658,7 @@ template <int M, bool LP> static int launch_w(Ctx *c, const DstArgs &a) {
     return ring ? launch_wr<M, LP>(c, a) : launch_wp<M, LP>(c, a);
 }
 
-// LP: single-precision arithmetic where the persistent-warp kernels serve (n + 1 = 64 .. 1024);
+// LP: single-precision arithmetic where the persistent-warp kernels serve (n + 1 = 64 .. 2048);
 // the other kernels compute in FP64 either way.
 template <bool IS, bool OS, bool LP = false> static int launch_dispatch(Ctx *c, int n, const DstArgs &a) {
     if (n < 1) { set_error("DST length must be >= 1 (got %d)", n); return HH_ERR_INVALID; }
@@ -1576,8 +1675,8 @@ template <bool IS, bool OS, bool LP = false> static int launch_dispatch(Ctx *c, 
         case 256: return launch_w<256, LP>(c, a);
         case 512: return launch_w<512, LP>(c, a);
         case 1024: return launch_w<1024, LP>(c, a);
-        case 2048: // two warps per line (FP64 only); rows_kernel 2 keeps the Stockham kernel below
-            if (!LP && a.rows_kernel != 2) return launch_w2<2048>(c, a);
+        case 2048: // two warps per line; rows_kernel 2 keeps the (FP64) Stockham kernel below
+            if (a.rows_kernel != 2) return launch_w2<2048, LP>(c, a);
             break;
         default: break;
         }

@@ -102,12 +102,38 @@ def test_refined_solve_reaches_tolerance(ctx, oracle, dim, n, order, k, batch):
     plan.solve(rhs, plain, batch)
     ctx.synchronize()
     assert rel_err(u.cpu().numpy(), plain.cpu().numpy()) < 1e-8
-    if n + 1 in (64, 128, 256, 512, 1024):
+    if n + 1 in (64, 128, 256, 512, 1024, 2048):
         assert iters >= 1  # single-precision transforms alone do not reach 1e-10
     u0 = torch.empty_like(rhs)
     it0, rr0 = plan.solve_refined(rhs, u0, batch, tol=1e-10, max_iter=0)
-    assert it0 == 0 and (rr0 > 1e-10 or n + 1 not in (64, 128, 256, 512, 1024))
+    assert it0 == 0 and (rr0 > 1e-10 or n + 1 not in (64, 128, 256, 512, 1024, 2048))
     plan.close()
+
+
+@pytest.mark.parametrize("k", [10.0, 100.0, 400.0])
+def test_refined_solve_2047_against_oracle_and_exact(ctx, oracle, k):
+    """The refined form at 2D N = 2047, order 6 (the mixed-precision configuration's size and
+    wavenumbers; k = 400 makes the lines lose diagonal dominance), on the right-hand side the
+    oracle assembles from a seeded 8-mode source: the 2048-point transforms run in
+    single-precision arithmetic, so at least one correction is needed; the result reaches the
+    1e-10 residual and agrees with the oracle's FP64 solution, and with the manufactured exact
+    solution as well as the oracle does (both to 1e-8 relative: the residual bound times the
+    lines' conditioning)."""
+    torch = pytest.importorskip("torch")
+    n, order = 2047, 6
+    modes = W.sine_modes(3000, 8, 20)
+    f_ext = W.source_2d(n, modes, fast=True)
+    ref = oracle.pipeline_2d(n, order, k, f_ext)
+    rhs = torch.from_numpy(np.ascontiguousarray(ref["rhs"].reshape(1, n, n))).cuda()
+    u = torch.empty_like(rhs)
+    plan = hh.Plan.helmholtz(ctx, 2, n, order, k)
+    iters, rr = plan.solve_refined(rhs, u, 1, tol=1e-10, max_iter=10)
+    plan.close()
+    got = u.cpu().numpy()[0]
+    assert iters >= 1 and rr <= 1e-10, (iters, rr)
+    assert rel_err(got, ref["sol"]) < 1e-8
+    exact = W.exact_2d(n, modes, k)
+    assert abs(rel_err(got, exact) - rel_err(ref["sol"], exact)) < 1e-8
 
 
 def test_refined_solve_argument_checks(ctx):
