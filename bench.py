@@ -187,8 +187,9 @@ def cpu_baseline(gpu_solve=None, max_seconds: float = 25.0, max_rhs: int = 12) -
 def cpu_check_secondary() -> dict:
     """CPU-baseline leg for the secondary configurations, one right-hand side each: the 3D
     N=255 order-6 k=30 solve through the oracle restatement (one core: the reference's 3D CPU path
-    has no threads) and the 2D N=2047 order-6 k=400 solve through the reference's own C path
-    (all cores), each timed and compared with the GPU's solution of the same right-hand side."""
+    has no threads), the 2D N=2047 order-6 k=400 solve through the reference's own C path (all
+    cores) and the README case (2D N=100 order 6 k=10, one core), each timed and compared with the
+    GPU's solution of the same right-hand side."""
     from hackathon_b200 import workload as W
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     out = {}
@@ -220,6 +221,24 @@ def cpu_check_secondary() -> dict:
         u = FIRST_RHS["2d_n2047_o6_b16"][400.0]
         out["2d_n2047_o6_k400"] = {"cpu_seconds_per_solve": dt, "cores": cores, "kind": kind,
                                    "rel_err_gpu_vs_oracle": float(np.abs(u - ref).max() / np.abs(ref).max())}
+    if "2d_n100_o6_k10_b1" in FIRST_RHS:
+        f = W.source_2d(100, W.sine_modes(3000, 8, 20), fast=True)
+        try:
+            from oracle import Reference2D
+            ref2 = Reference2D()
+            t0 = time.perf_counter()
+            with _quiet_stdout():
+                run = ref2.pipeline(100, 6, 10.0, f, threads=1)
+            dt, kind = time.perf_counter() - t0, "reference"
+            ref = run.arrays["sol"].reshape(100, 100)
+        except Exception:
+            from oracle import Oracle
+            t0 = time.perf_counter()
+            ref = Oracle().pipeline_2d(100, 6, 10.0, f)["sol"]
+            dt, kind = time.perf_counter() - t0, "port"
+        u = FIRST_RHS["2d_n100_o6_k10_b1"][10.0]
+        out["2d_n100_o6_k10"] = {"cpu_seconds_per_solve": dt, "cores": 1, "kind": kind,
+                                 "rel_err_gpu_vs_oracle": float(np.abs(u - ref).max() / np.abs(ref).max())}
     return out
 
 
@@ -295,11 +314,13 @@ FIRST_RHS: dict = {}  # secondary configuration -> {k: solution of its first rig
 
 def secondary_configs(hh, ctx, st, torch) -> dict:
     """Device-resident solves/s of the other plain-FP64 configurations named with the metric:
-    3D N=255 order 6 k=30 batch 4 (16 sine modes, p,q,r <= 64) and 2D N=2047 order 6 batch 16,
-    k in {10, 100, 400} (8 modes, p,q <= 20).  Short CUDA-event timings of captured graphs."""
+    3D N=255 order 6 k=30 batch 4 (16 sine modes, p,q,r <= 64), 2D N=2047 order 6 batch 16,
+    k in {10, 100, 400} (8 modes, p,q <= 20), and the README case, 2D N=100 order 6 k=10, one
+    right-hand side of 8 modes (p,q <= 20).  Short CUDA-event timings of captured graphs."""
     from hackathon_b200 import workload as W
     out = {}
-    cases = [("3d_n255_o6_k30_b4", 3, 255, 6, [30.0], 4), ("2d_n2047_o6_b16", 2, 2047, 6, [10.0, 100.0, 400.0], 16)]
+    cases = [("3d_n255_o6_k30_b4", 3, 255, 6, [30.0], 4), ("2d_n2047_o6_b16", 2, 2047, 6, [10.0, 100.0, 400.0], 16),
+             ("2d_n100_o6_k10_b1", 2, 100, 6, [10.0], 1)]
     for name, dim, n, order, ks, batch in cases:
         if dim == 3:
             f_host = np.stack([W.source_3d(n, W.sine_modes(2000 + b, 16, 64, dim=3))[1:-1, 1:-1, 1:-1]
