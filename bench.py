@@ -726,7 +726,7 @@ def main():
 
     # end to end through the public host API (pinned host buffers, copies inside the region)
     io_bytes = batch * N * N * 16
-    e2e_steps, e2e_value = 0, None
+    e2e_steps, e2e_value, e2e_copy = 0, None, None
     if not args.no_e2e:
         pin_in = torch.from_numpy(f_host).pin_memory()
         pin_out = torch.empty_like(pin_in).pin_memory()
@@ -743,6 +743,25 @@ def main():
         if world > 1:
             dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
         e2e_value = world * batch * e2e_steps / float(e2e_s.item())
+        # the transfer bound beside it: the same pinned buffers copied in and out at the same time
+        # (two streams, one device buffer each), no solve; e2e / this = the fraction of the PCIe
+        # ceiling the end-to-end path reaches
+        d_in, d_out = torch.empty_like(pin_in, device="cuda"), torch.empty_like(pin_in, device="cuda")
+        s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+        for rep in range(3):
+            if rep == 1:
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+            with torch.cuda.stream(s_in):
+                d_in.copy_(pin_in, non_blocking=True)
+            with torch.cuda.stream(s_out):
+                pin_out.copy_(d_out, non_blocking=True)
+        torch.cuda.synchronize()
+        copy_s = (time.perf_counter() - t0) / 2
+        e2e_copy = {"both_directions_gbs": 2 * io_bytes / copy_s / 1e9, "copy_only_solves_per_s": batch / copy_s,
+                    "e2e_frac_of_copy_bound": e2e_value / (world * batch / copy_s)}
+        del d_in, d_out
+        torch.cuda.empty_cache()
 
     if rank == 0:
         line = {
@@ -761,7 +780,7 @@ def main():
                          "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "whole_step_achieved": 3 * BYTES_PER_POINT_STAGE * pts * args.steps / (ms / 1000.0) / 1e9},
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": io_bytes,
-                    "d2h_bytes_per_step": io_bytes, "steps": e2e_steps},
+                    "d2h_bytes_per_step": io_bytes, "steps": e2e_steps, "transfer_bound": e2e_copy},
             "gpu_launches": launches,
             "timing": "CUDA events on the launch stream around CUDA-graph replays (one graph per (order, k))",
             "clocks": dict(clk.summary(), window="0.5 s of the same graph replays just before the timed "
