@@ -124,7 +124,8 @@ struct Plan {
     int      variant = 0;        // line-solve kernel: 0/1 general (512x1, 256x2), 2..6 symmetric
     long     slab = 0;           // 3D: planes per slab of the transform passes (0: the whole batch)
     int      col_kernel = 0;     // 3D column DST: 0 CTA tiles of 8 swizzled columns, 1 per-warp tiles
-    int      rows_kernel = 0;    // rows DST (n + 1 = 64 .. 1024): 0 default, 1 CTA ring, 2 per-warp buffers
+    int      rows_kernel = 0;    // rows DST (n + 1 = 64 .. 1024): 0 default, 1 CTA ring, 2 per-warp buffers;
+                                 // (n + 1 = 2048): 0, 1 two warps per line, 2 the Stockham kernel
     bool     sym = false;        // const_rows and sub == super on every line (constant k)
     bool     pf_ok = false;      // order-6 partial fractions well conditioned on every line
     double2 *subt = nullptr, *diagt = nullptr; // sub/diagonal row tables (4 * rows each)
@@ -140,9 +141,9 @@ struct Plan {
 };
 
 // lp: single-precision arithmetic (the refined solve's corrections) where the persistent-warp
-// kernels serve (n + 1 = 64 .. 1024); FP64 otherwise
+// kernels serve (n + 1 = 64 .. 2048); FP64 otherwise
 // rows_kernel (n + 1 = 64 .. 1024): 0 the length's default, 1 the CTA ring of line buffers, 2
-// per-warp line buffers
+// per-warp line buffers; (n + 1 = 2048): 0 and 1 two warps per line, 2 the Stockham kernel
 int launch_dst_rows(Ctx *c, int n, long rows, const double2 *in, long in_ld, double2 *out, long out_ld,
                     bool lp = false, int rows_kernel = 0);
 // kern: 0 = CTA tiles of 8 swizzled columns where the length allows, 1 = per-warp tiles of LPW columns
