@@ -985,6 +985,25 @@ extern "C" int hh_solve_refined(hh_plan *pl, const double *rhs, double *sol, int
         HH_TRY(launch_line_solve(&p, out, out, batch, 0));
         return transform_inverse(p, out, batch, true);
     };
+    // a correction u <- u - S(w): the last (rows) pass of the inverse transform subtracts its
+    // result from u as it stores, where the rows kernel has that form; else a separate update
+    auto correct = [&]() -> int {
+        if (!rows_update_supported(p.nx, p.rows_kernel)) {
+            HH_TRY(low_solve(w, w));
+            return launch_axpy(c, u, w, -1.0, need);
+        }
+        HH_TRY(transform_forward(p, w, w, batch, true));
+        HH_TRY(launch_line_solve(&p, w, w, batch, 0));
+        if (p.dim == 2) return launch_dst_rows_update(c, p.nx, (long)p.ny * batch, w, p.nx, u, p.nx, p.rows_kernel);
+        const long plane = (long)p.nx * p.ny, planes = (long)p.nz * batch, sp = slab_planes(p, planes);
+        for (long p0 = 0; p0 < planes; p0 += sp) {
+            const long np = std::min(sp, planes - p0);
+            HH_TRY(launch_dst_cols(c, p.ny, p.nx, np, w + p0 * plane, p.nx, plane, w + p0 * plane, true, p.col_kernel));
+            HH_TRY(launch_dst_rows_update(c, p.nx, (long)p.ny * np, w + p0 * plane, p.nx, u + p0 * plane, p.nx,
+                                          p.rows_kernel));
+        }
+        return HH_OK;
+    };
     HH_TRY(low_solve(f, u));
     int    k = 0;
     double rr = 0.0;
@@ -998,8 +1017,7 @@ extern "C" int hh_solve_refined(hh_plan *pl, const double *rhs, double *sol, int
         memcpy(v, h, sizeof(v));
         rr = v[1] > 0.0 ? v[0] / v[1] : 0.0;
         if (rr <= tol || k >= max_iter) break;
-        HH_TRY(low_solve(w, w));
-        HH_TRY(launch_axpy(c, u, w, -1.0, need));
+        HH_TRY(correct());
         k++;
     }
     if (iters) *iters = k;

@@ -736,7 +736,8 @@ __device__ __forceinline__ void w_transform_lp(XLoad xload, double2 *buf, int l,
 constexpr uint32_t kInjectBytes = 16;
 constexpr long     kInjectPolls = 1L << 12;
 
-template <int M, bool LP = false>
+// UPD (the refined solve's correction, single-precision transforms): out <- out - result
+template <int M, bool LP = false, bool UPD = false>
 __global__ void __launch_bounds__(32 * WCfg<M>::WPC, WCfg<M>::MINB)
     k_dst1_w(const double2 *in, double2 *out, long nlines, long nplanes, long in_ld, long out_ld, long in_plane,
              long out_plane, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err, int *inj) {
@@ -805,7 +806,10 @@ __global__ void __launch_bounds__(32 * WCfg<M>::WPC, WCfg<M>::MINB)
 #pragma unroll
             for (int q = 0; q < M / TL; q++) {
                 const int p = l + TL * q;
-                if (p < N) dst[p] = buf[(K2 + 1) * (p / K2) + p % K2];
+                if (p < N) {
+                    const double2 o = buf[(K2 + 1) * (p / K2) + p % K2];
+                    dst[p] = UPD ? csub(dst[p], o) : o;
+                }
             }
         }
         // the buffer set is free again: bring in the group after next (every lane orders its
@@ -842,7 +846,7 @@ template <int M> struct WRing {
     static_assert(NS * 8 + NS * 4 <= 128, "barriers and counters fit in front of the buffers");
 };
 
-template <int M, bool LP = false>
+template <int M, bool LP = false, bool UPD = false>
 __global__ void __launch_bounds__(32 * WCfg<M>::RWPC, 2)
     k_dst1_wr(const double2 *in, double2 *out, long nlines, long nplanes, long in_ld, long out_ld, long in_plane,
               long out_plane, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
@@ -918,7 +922,10 @@ __global__ void __launch_bounds__(32 * WCfg<M>::RWPC, 2)
 #pragma unroll
             for (int q = 0; q < M / TL; q++) {
                 const int p = l + TL * q;
-                if (p < N) dst[p] = buf[(K2 + 1) * (p / K2) + p % K2];
+                if (p < N) {
+                    const double2 o = buf[(K2 + 1) * (p / K2) + p % K2];
+                    dst[p] = UPD ? csub(dst[p], o) : o;
+                }
             }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // reads before the refill
@@ -1066,7 +1073,7 @@ __device__ __forceinline__ void w2_transform_lp(double2 *buf, int l, int h, int 
     team_sync(bid); // outputs complete
 }
 
-template <int M, bool LP = false>
+template <int M, bool LP = false, bool UPD = false>
 __global__ void __launch_bounds__(64 * W2Geom<M>::TPC, 1)
     k_dst1_w2(const double2 *in, double2 *out, long nlines, long nplanes, long in_ld, long out_ld, long in_plane,
               long out_plane, const double2 *__restrict__ tw, const double *__restrict__ sn, int *err) {
@@ -1222,7 +1229,10 @@ __global__ void __launch_bounds__(64 * W2Geom<M>::TPC, 1)
 #pragma unroll
         for (int q = 0; q < M / TL; q++) {
             const int p = l + TL * q;
-            if (p < N) dst[p] = buf[(K2 + 1) * (p / K2) + p % K2];
+            if (p < N) {
+                const double2 o = buf[(K2 + 1) * (p / K2) + p % K2];
+                dst[p] = UPD ? csub(dst[p], o) : o;
+            }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // reads before the refill
         team_sync(bid);
@@ -1592,39 +1602,39 @@ template <int M, bool IS, bool OS> static int launch_fft(Ctx *c, const DstArgs &
     return HH_OK;
 }
 
-template <int M, bool LP> static int launch_wr(Ctx *c, const DstArgs &a) {
+template <int M, bool LP, bool UPD = false> static int launch_wr(Ctx *c, const DstArgs &a) {
     using G = WGeom<M>;
     using RG = WRing<M>;
     const double2 *tw;
     const double  *sn;
     HH_TRY(tables_for(c, M, &tw, &sn));
-    HH_CUDA(cudaFuncSetAttribute(k_dst1_wr<M, LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, RG::SMEM));
+    HH_CUDA(cudaFuncSetAttribute(k_dst1_wr<M, LP, UPD>, cudaFuncAttributeMaxDynamicSharedMemorySize, RG::SMEM));
     int dev = 0, sms = 148, per_sm = 0;
     HH_CUDA(cudaGetDevice(&dev));
     HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dst1_wr<M, LP>, 32 * RG::WPC, RG::SMEM));
+    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dst1_wr<M, LP, UPD>, 32 * RG::WPC, RG::SMEM));
     const long groups = (a.nlines * a.planes + G::LPW - 1) / G::LPW;
     const long ctas = std::min<long>((groups + RG::WPC - 1) / RG::WPC, (long)std::max(1, per_sm) * sms);
-    k_dst1_wr<M, LP><<<(unsigned)ctas, 32 * RG::WPC, RG::SMEM, c->stream>>>(
+    k_dst1_wr<M, LP, UPD><<<(unsigned)ctas, 32 * RG::WPC, RG::SMEM, c->stream>>>(
         a.in, a.out, a.nlines, a.planes, a.in_ld, a.out_ld, a.in_plane, a.out_plane, tw, sn, c->err_word);
     HH_CUDA(cudaGetLastError());
     c->launches++;
     return HH_OK;
 }
 
-template <int M, bool LP> static int launch_wp(Ctx *c, const DstArgs &a) {
+template <int M, bool LP, bool UPD = false> static int launch_wp(Ctx *c, const DstArgs &a) {
     using G = WGeom<M>;
     const double2 *tw;
     const double  *sn;
     HH_TRY(tables_for(c, M, &tw, &sn));
-    HH_CUDA(cudaFuncSetAttribute(k_dst1_w<M, LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
+    HH_CUDA(cudaFuncSetAttribute(k_dst1_w<M, LP, UPD>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
     int dev = 0, sms = 148, per_sm = 0;
     HH_CUDA(cudaGetDevice(&dev));
     HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dst1_w<M, LP>, 32 * G::WPC, G::SMEM));
+    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dst1_w<M, LP, UPD>, 32 * G::WPC, G::SMEM));
     const long groups = (a.nlines * a.planes + G::LPW - 1) / G::LPW;
     const long ctas = std::min<long>((groups + G::WPC - 1) / G::WPC, (long)std::max(1, per_sm) * sms);
-    k_dst1_w<M, LP><<<(unsigned)ctas, 32 * G::WPC, G::SMEM, c->stream>>>(a.in, a.out, a.nlines, a.planes, a.in_ld, a.out_ld,
+    k_dst1_w<M, LP, UPD><<<(unsigned)ctas, 32 * G::WPC, G::SMEM, c->stream>>>(a.in, a.out, a.nlines, a.planes, a.in_ld, a.out_ld,
                                                                      a.in_plane, a.out_plane, tw, sn, c->err_word,
                                                                      c->inject_word);
     HH_CUDA(cudaGetLastError());
@@ -1632,19 +1642,19 @@ template <int M, bool LP> static int launch_wp(Ctx *c, const DstArgs &a) {
     return HH_OK;
 }
 
-template <int M, bool LP> static int launch_w2(Ctx *c, const DstArgs &a) {
+template <int M, bool LP, bool UPD = false> static int launch_w2(Ctx *c, const DstArgs &a) {
     using G = W2Geom<M>;
     const double2 *tw;
     const double  *sn;
     HH_TRY(tables_for(c, M, &tw, &sn));
-    HH_CUDA(cudaFuncSetAttribute(k_dst1_w2<M, LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
+    HH_CUDA(cudaFuncSetAttribute(k_dst1_w2<M, LP, UPD>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM));
     int dev = 0, sms = 148, per_sm = 0;
     HH_CUDA(cudaGetDevice(&dev));
     HH_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dst1_w2<M, LP>, 64 * G::TPC, G::SMEM));
+    HH_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dst1_w2<M, LP, UPD>, 64 * G::TPC, G::SMEM));
     const long lines = a.nlines * a.planes;
     const long ctas = std::min<long>((lines + G::TPC - 1) / G::TPC, (long)std::max(1, per_sm) * sms);
-    k_dst1_w2<M, LP><<<(unsigned)ctas, 64 * G::TPC, G::SMEM, c->stream>>>(a.in, a.out, a.nlines, a.planes, a.in_ld,
+    k_dst1_w2<M, LP, UPD><<<(unsigned)ctas, 64 * G::TPC, G::SMEM, c->stream>>>(a.in, a.out, a.nlines, a.planes, a.in_ld,
                                                                         a.out_ld, a.in_plane, a.out_plane, tw, sn,
                                                                         c->err_word);
     HH_CUDA(cudaGetLastError());
@@ -1653,14 +1663,15 @@ template <int M, bool LP> static int launch_w2(Ctx *c, const DstArgs &a) {
 }
 
 // rows kernel: a.rows_kernel 1 = the CTA ring, 2 = per-warp buffers, 0 = the length's default
-template <int M, bool LP> static int launch_w(Ctx *c, const DstArgs &a) {
+template <int M, bool LP, bool UPD = false> static int launch_w(Ctx *c, const DstArgs &a) {
     const bool ring = a.rows_kernel == 0 ? (bool)WCfg<M>::RING : a.rows_kernel == 1;
-    return ring ? launch_wr<M, LP>(c, a) : launch_wp<M, LP>(c, a);
+    return ring ? launch_wr<M, LP, UPD>(c, a) : launch_wp<M, LP, UPD>(c, a);
 }
 
 // LP: single-precision arithmetic where the persistent-warp kernels serve (n + 1 = 64 .. 2048);
 // the other kernels compute in FP64 either way.
-template <bool IS, bool OS, bool LP = false> static int launch_dispatch(Ctx *c, int n, const DstArgs &a) {
+// UPD: out <- out - result, only where the persistent-warp kernels serve (rows_update_supported)
+template <bool IS, bool OS, bool LP = false, bool UPD = false> static int launch_dispatch(Ctx *c, int n, const DstArgs &a) {
     if (n < 1) { set_error("DST length must be >= 1 (got %d)", n); return HH_ERR_INVALID; }
     if (a.nlines <= 0 || a.planes <= 0) return HH_OK;
     if (a.planes > 65535) { set_error("DST: too many planes (%ld)", a.planes); return HH_ERR_INVALID; }
@@ -1670,16 +1681,20 @@ template <bool IS, bool OS, bool LP = false> static int launch_dispatch(Ctx *c, 
     }
     if (!IS && !OS) {
         switch (n + 1) { // contiguous rows: persistent-warp kernels
-        case 64: return launch_w<64, LP>(c, a);
-        case 128: return launch_w<128, LP>(c, a);
-        case 256: return launch_w<256, LP>(c, a);
-        case 512: return launch_w<512, LP>(c, a);
-        case 1024: return launch_w<1024, LP>(c, a);
+        case 64: return launch_w<64, LP, UPD>(c, a);
+        case 128: return launch_w<128, LP, UPD>(c, a);
+        case 256: return launch_w<256, LP, UPD>(c, a);
+        case 512: return launch_w<512, LP, UPD>(c, a);
+        case 1024: return launch_w<1024, LP, UPD>(c, a);
         case 2048: // two warps per line; rows_kernel 2 keeps the (FP64) Stockham kernel below
-            if (a.rows_kernel != 2) return launch_w2<2048, LP>(c, a);
+            if (a.rows_kernel != 2) return launch_w2<2048, LP, UPD>(c, a);
             break;
         default: break;
         }
+    }
+    if constexpr (UPD) {
+        set_error("DST length %d: no subtracting form for these kernels", n);
+        return HH_ERR_UNSUPPORTED;
     }
     switch (n + 1) {
     case 64: return launch_fft<64, IS, OS>(c, a);
@@ -1711,6 +1726,17 @@ template <bool IS, bool OS, bool LP = false> static int launch_dispatch(Ctx *c, 
     HH_CUDA(cudaGetLastError());
     c->launches++;
     return HH_OK;
+}
+
+bool rows_update_supported(int n, int rows_kernel) {
+    const int m = n + 1;
+    return (m >= 64 && m <= 1024 && (m & (m - 1)) == 0) || (m == 2048 && rows_kernel != 2);
+}
+
+int launch_dst_rows_update(Ctx *c, int n, long rows, const double2 *in, long in_ld, double2 *out, long out_ld,
+                           int rows_kernel) {
+    DstArgs a{in, out, rows, 1, in_ld, out_ld, 0, 0, rows_kernel};
+    return launch_dispatch<false, false, true, true>(c, n, a);
 }
 
 int launch_dst_rows(Ctx *c, int n, long rows, const double2 *in, long in_ld, double2 *out, long out_ld, bool lp,

@@ -146,6 +146,12 @@ struct Plan {
 // per-warp line buffers; (n + 1 = 2048): 0 and 1 two warps per line, 2 the Stockham kernel
 int launch_dst_rows(Ctx *c, int n, long rows, const double2 *in, long in_ld, double2 *out, long out_ld,
                     bool lp = false, int rows_kernel = 0);
+// The refined solve's correction: the single-precision rows transform of `in` subtracted from
+// `out` (out <- out - DST(in)), for the lengths rows_update_supported admits (n + 1 = 64 .. 1024,
+// and 2048 unless rows_kernel is 2); HH_ERR_UNSUPPORTED, before any launch, otherwise.
+bool rows_update_supported(int n, int rows_kernel);
+int  launch_dst_rows_update(Ctx *c, int n, long rows, const double2 *in, long in_ld, double2 *out, long out_ld,
+                            int rows_kernel);
 // kern: 0 = CTA tiles of 8 swizzled columns where the length allows, 1 = per-warp tiles of LPW columns
 int launch_dst_cols(Ctx *c, int n, long ncols, long planes, const double2 *in, long ld, long plane_stride,
                     double2 *out, bool lp = false, int kern = 0);
