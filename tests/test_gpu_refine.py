@@ -41,8 +41,10 @@ def test_residual_2d_matches_oracle(ctx, oracle, n, order, k):
     plan.close()
 
 
-@pytest.mark.parametrize("n,order,k", [(15, 6, 30.0), (31, 4, 10.0)])
+@pytest.mark.parametrize("n,order,k", [(15, 6, 30.0), (31, 4, 10.0), (100, 6, 20.0), (127, 2, 30.0)])
 def test_residual_3d_matches_oracle(ctx, oracle, n, order, k):
+    """The tiled residual (32 x 8 tiles of the (x, y) plane marching through 64 layers): partial
+    tiles at n = 100 and 15, and more than one chunk of layers at n = 100 and 127."""
     torch = pytest.importorskip("torch")
     m = W.sine_modes(n + order, 16, min(n, 64), dim=3)
     ref = oracle.pipeline_3d(n, order, k, W.source_3d(n, m))
