@@ -575,7 +575,8 @@ def serve_run(hh, torch, seconds: float = 2.0, rate: float = 2000.0, seed: int =
 
 def serving_block(hh, torch, seconds: float = 1.0, rate: float = 2000.0) -> dict:
     """The configured stream, then the same mix at 80 % of the request rate the device completed
-    on it (latency under a load it sustains)."""
+    on it (latency under a load it sustains, close to saturation for this mix) and at 50 % (latency
+    with headroom)."""
     sizes = [(2, n) for n in SERVE_2D] + [(3, n) for n in SERVE_3D]
     bufs = {}
     for i, (dim, n) in enumerate(sizes):
@@ -584,9 +585,10 @@ def serving_block(hh, torch, seconds: float = 1.0, rate: float = 2000.0) -> dict
     pre = serve_pretune(hh)
     res = serve_run(hh, torch, seconds=seconds, rate=rate, bufs=bufs)
     sus = serve_run(hh, torch, seconds=seconds, rate=0.8 * res["requests_per_s"], seed=6, bufs=bufs)
+    half = serve_run(hh, torch, seconds=seconds, rate=0.5 * res["requests_per_s"], seed=7, bufs=bufs)
     del bufs
     torch.cuda.empty_cache()
-    return {"configured": res, "sustainable": sus, "pretune_s": pre}
+    return {"configured": res, "sustainable": sus, "half_load": half, "pretune_s": pre}
 
 
 def main():

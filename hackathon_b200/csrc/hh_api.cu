@@ -392,10 +392,13 @@ static int plan_factor(hh_plan *pl, const std::vector<double2> &sub, const std::
             const double2 a = tb[0], b = tb[(size_t)p.rows], c = tb[2 * (size_t)p.rows], d = tb[3 * (size_t)p.rows];
             return make_double2(((a.x * m0 + b.x * m1) + c.x * m2) + d.x, ((a.y * m0 + b.y * m1) + c.y * m2) + d.y);
         };
+        // |10 s - d| >= |s|, |d| / 4 and |s| > 1e-6 |d|, on squared moduli (one line of a 255^3
+        // plan is one of 65025: three hypot calls per line cost milliseconds of set-up)
         const double2 s = line_value(sub), d = line_value(dia);
-        const double  num = std::hypot(10.0 * s.x - d.x, 10.0 * s.y - d.y);
-        const double  as = std::hypot(s.x, s.y), ad = std::hypot(d.x, d.y);
-        p.pf_ok = num >= 0.25 * std::max(as, ad) && as > 1e-6 * ad;
+        const double  ex = 10.0 * s.x - d.x, ey = 10.0 * s.y - d.y;
+        const double  num2 = ex * ex + ey * ey;
+        const double  as2 = s.x * s.x + s.y * s.y, ad2 = d.x * d.x + d.y * d.y;
+        p.pf_ok = num2 >= 0.0625 * std::max(as2, ad2) && as2 > 1e-12 * ad2;
     }
     if (p.sym) p.variant = sym_default_variant(p.rows);
     // tables are [4][prow], zero past the last row (neutral rows in the solve)
@@ -481,11 +484,12 @@ extern "C" int hh_plan3d_create(hh_ctx *x, int nx, int ny, int nz, const double 
     int rc = plan_alloc(pl);
     if (rc != HH_OK) { plan_free(pl); delete pl; return rc; }
     // eigenvalue products per (i,j) line, as 3D LU.c:31-44
-    std::vector<double> mu(3 * (size_t)p.lines);
+    std::vector<double> mu(3 * (size_t)p.lines), exs((size_t)nx);
+    for (int i = 0; i < nx; i++) exs[(size_t)i] = 2.0 * cos((i + 1) * M_PI / (nx + 1));
     for (int j = 0; j < ny; j++) {
         const double ey = 2.0 * cos((j + 1) * M_PI / (ny + 1));
         for (int i = 0; i < nx; i++) {
-            const double ex = 2.0 * cos((i + 1) * M_PI / (nx + 1));
+            const double ex = exs[(size_t)i];
             const long   q = i + (long)j * nx;
             mu[q] = ex * ey;
             mu[p.lines + q] = ex;
