@@ -37,6 +37,9 @@ namespace {
 
 constexpr int  kMergeRhs = 64;          // right-hand sides in one merged batch at most
 constexpr long kMergePoints = 1L << 22; // requests with more points than this run on their own
+// memory the pool reserves at creation (up to the budget): a fresh pool grows as plans and
+// staging arrive, and a growth can stall the dispatcher for tens of milliseconds
+constexpr size_t kReserveBytes = 64ull << 30;
 
 using Key = std::tuple<int, int, int, double, double>; // dim, n, order, k_re, k_im
 
@@ -428,6 +431,16 @@ extern "C" int hh_server_create(int device, size_t budget, int streams, hh_serve
     if (e == cudaSuccess) {
         unsigned long long keep = (unsigned long long)budget; // keep freed staging in the pool up to the budget
         e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    if (e == cudaSuccess) { // reserve the pool's memory up front: one allocation, freed at once
+        cudaStream_t ws = nullptr;
+        void        *w = nullptr;
+        e = cudaStreamCreateWithFlags(&ws, cudaStreamNonBlocking);
+        const size_t wb = std::min(budget, kReserveBytes);
+        if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&w, wb, s->pool, ws);
+        if (e == cudaSuccess) e = cudaFreeAsync(w, ws);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ws);
+        if (ws) cudaStreamDestroy(ws);
     }
     if (e == cudaSuccess) e = cudaHostAlloc((void **)&s->flags, sizeof(int) * 64, cudaHostAllocDefault);
     if (e == cudaSuccess) memset(s->flags, 0, sizeof(int) * 64);

@@ -270,7 +270,10 @@ int hh_coefficients3d(int n, int order, double k_re, double k_im, double *const 
  *    (hh_solve_source_multi);
  *  - admission: a batch starts while plans plus in-flight staging fit the HBM budget, otherwise
  *    it waits for running batches; a request that can never fit fails with HH_ERR_NOMEM;
- *  - batches go round-robin to `streams` CUDA streams, so requests overlap on the device.
+ *  - batches go round-robin to `streams` CUDA streams, so requests overlap on the device;
+ *  - memory: the server's stream-ordered pool reserves min(budget, 64 GB) of device memory when
+ *    the server is created and keeps it until hh_server_destroy (a fresh pool growing under load
+ *    stalls the dispatcher).
  * Each result is bitwise the result of hh_solve_source on a plan of the same problem.  Host
  * buffers should be pinned for copies to overlap; device buffers (on_device = 1) are used
  * directly when a request runs alone.  Buffers must stay valid until hh_server_wait returns. */
