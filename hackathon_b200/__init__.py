@@ -72,6 +72,7 @@ SIGNATURES = {
     "hh_plan3d_create": (_i, [_vp, _i, _i, _i, C.POINTER(_vp), C.POINTER(_vp)]),
     "hh_plan2d_create_helmholtz": (_i, [_vp, _i, _i, _d, _d, C.POINTER(_vp)]),
     "hh_plan3d_create_helmholtz": (_i, [_vp, _i, _i, _d, _d, C.POINTER(_vp)]),
+    "hh_plan3d_create_helmholtz_lines": (_i, [_vp, _i, _i, _d, _d, _l, _l, C.POINTER(_vp)]),
     "hh_plan_destroy": (_i, [_vp]),
     "hh_plan_field_size": (_l, [_vp]),
     "hh_plan_tune": (_i, [_vp, _i]),
@@ -92,6 +93,7 @@ SIGNATURES = {
     "hh_solve_host": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source_host": (_i, [_vp, _vp, _vp, _i]),
+    "hh_solve_lines": (_i, [_vp, _vp, _vp, _i, _i]),
     "hh_solve_source_host_noalloc": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source_multi": (_i, [C.POINTER(_vp), C.POINTER(_i), _i, _vp, _vp]),
     "hh_rhs2d": (_i, [_vp, C.POINTER(Rhs2DData), _vp]),
@@ -249,6 +251,16 @@ class Plan:
         check(lib().hh_plan3d_create_helmholtz(ctx.h, n, order, k.real, k.imag, C.byref(p)), "helmholtz3d")
         return cls(ctx, p, 3, (n, n, n))
 
+    @classmethod
+    def helmholtz_lines(cls, ctx: Context, n: int, order: int, k: complex, q0: int, q1: int):
+        """The z line solves of lines [q0, q1) of a 3D Helmholtz plan (a rank's pencil,
+        hh_plan3d_create_helmholtz_lines); fields are laid out [z][q - q0]."""
+        p = _vp()
+        k = complex(k)
+        check(lib().hh_plan3d_create_helmholtz_lines(ctx.h, n, order, k.real, k.imag, q0, q1, C.byref(p)),
+              "hh_plan3d_create_helmholtz_lines")
+        return cls(ctx, p, 3, (n, q1 - q0))
+
     def close(self):
         if self.h and self.ctx.h:
             lib().hh_plan_destroy(self.h)
@@ -313,6 +325,11 @@ class Plan:
 
     def solve_source(self, f, u, batch: int = 1):
         check(lib().hh_solve_source(self.h, _addr(f), _addr(u), batch), "hh_solve_source")
+
+    def solve_lines(self, src, dst, batch: int = 1, fused: bool = True):
+        """The line solve alone on transformed fields (hh_solve_lines): fused = True for transformed
+        sources (the Helmholtz plans' compact operator), False for assembled right-hand sides."""
+        check(lib().hh_solve_lines(self.h, _addr(src), _addr(dst), batch, 1 if fused else 0), "hh_solve_lines")
 
     def solve_refined(self, rhs, sol, batch: int = 1, tol: float = 1e-10, max_iter: int = 10):
         """hh_solve_refined on device buffers; returns (corrections, relative residual)."""

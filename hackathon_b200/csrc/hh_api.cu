@@ -461,8 +461,11 @@ extern "C" int hh_plan2d_create(hh_ctx *x, int nx, int ny, const double *bp, con
     return HH_OK;
 }
 
-extern "C" int hh_plan3d_create(hh_ctx *x, int nx, int ny, int nz, const double *const coef[12], hh_plan **out) {
-    if (!x || !out || nx < 1 || ny < 1 || nz < 1 || !coef) {
+// A 3D plan over lines [q0, q1) of the nx * ny (i, j) lines, q = i + j nx: the whole field for
+// hh_plan3d_create, one rank's pencil for hh_plan3d_create_helmholtz_lines.
+static int plan3d_create_lines(hh_ctx *x, int nx, int ny, int nz, const double *const coef[12], long q0, long q1,
+                               hh_plan **out) {
+    if (!x || !out || nx < 1 || ny < 1 || nz < 1 || !coef || q0 < 0 || q1 <= q0 || q1 > (long)nx * ny) {
         set_error("hh_plan3d_create: invalid arguments");
         return HH_ERR_INVALID;
     }
@@ -477,24 +480,25 @@ extern "C" int hh_plan3d_create(hh_ctx *x, int nx, int ny, int nz, const double 
     p.nx = nx;
     p.ny = ny;
     p.nz = nz;
-    p.lines = nx * ny;
+    p.line0 = q0;
+    p.lines_only = q0 > 0 || q1 < (long)nx * ny;
+    p.lines = (int)(q1 - q0);
     p.rows = nz;
-    p.row_stride = (long)nx * ny;
-    p.field = (long)nx * ny * nz;
+    p.row_stride = p.lines;
+    p.field = (long)p.lines * nz;
     int rc = plan_alloc(pl);
     if (rc != HH_OK) { plan_free(pl); delete pl; return rc; }
     // eigenvalue products per (i,j) line, as 3D LU.c:31-44
-    std::vector<double> mu(3 * (size_t)p.lines), exs((size_t)nx);
+    std::vector<double> mu(3 * (size_t)p.lines), exs((size_t)nx), eys((size_t)ny);
     for (int i = 0; i < nx; i++) exs[(size_t)i] = 2.0 * cos((i + 1) * M_PI / (nx + 1));
-    for (int j = 0; j < ny; j++) {
-        const double ey = 2.0 * cos((j + 1) * M_PI / (ny + 1));
-        for (int i = 0; i < nx; i++) {
-            const double ex = exs[(size_t)i];
-            const long   q = i + (long)j * nx;
-            mu[q] = ex * ey;
-            mu[p.lines + q] = ex;
-            mu[2 * (size_t)p.lines + q] = ey;
-        }
+    for (int j = 0; j < ny; j++) eys[(size_t)j] = 2.0 * cos((j + 1) * M_PI / (ny + 1));
+    for (long q = q0; q < q1; q++) {
+        const int    i = (int)(q % nx), j = (int)(q / nx);
+        const double ey = eys[(size_t)j], ex = exs[(size_t)i];
+        const long   t = q - q0;
+        mu[(size_t)t] = ex * ey;
+        mu[p.lines + (size_t)t] = ex;
+        mu[2 * (size_t)p.lines + (size_t)t] = ey;
     }
     // coef order a,b,c,d,ap,bp,cp,dp,am,bm,cm,dm -> (corner, x-neighbour, y-neighbour, centre)
     std::vector<double2> sub(4 * (size_t)nz), dia(4 * (size_t)nz), sup(4 * (size_t)nz);
@@ -508,6 +512,10 @@ extern "C" int hh_plan3d_create(hh_ctx *x, int nx, int ny, int nz, const double 
     if (rc != HH_OK) { plan_free(pl); delete pl; return rc; }
     *out = pl;
     return HH_OK;
+}
+
+extern "C" int hh_plan3d_create(hh_ctx *x, int nx, int ny, int nz, const double *const coef[12], hh_plan **out) {
+    return plan3d_create_lines(x, nx, ny, nz, coef, 0, (long)nx * ny, out);
 }
 
 extern "C" int hh_plan2d_create_helmholtz(hh_ctx *x, int n, int order, double kr, double ki, hh_plan **out) {
@@ -527,7 +535,9 @@ extern "C" int hh_plan2d_create_helmholtz(hh_ctx *x, int n, int order, double kr
     return HH_OK;
 }
 
-extern "C" int hh_plan3d_create_helmholtz(hh_ctx *x, int n, int order, double kr, double ki, hh_plan **out) {
+extern "C" int hh_plan3d_create_helmholtz_lines(hh_ctx *x, int n, int order, double kr, double ki, long q0, long q1,
+                                                hh_plan **out) {
+    if (n < 1) { set_error("hh_plan3d_create_helmholtz: n = %d", n); return HH_ERR_INVALID; }
     std::vector<double> buf(12 * 2 * (size_t)n);
     double *arr[12];
     for (int t = 0; t < 12; t++) arr[t] = buf.data() + t * 2 * (size_t)n;
@@ -535,7 +545,7 @@ extern "C" int hh_plan3d_create_helmholtz(hh_ctx *x, int n, int order, double kr
     if (rc != HH_OK) { set_error("hh_plan3d_create_helmholtz: order must be 2, 4 or 6"); return rc; }
     const double *carr[12];
     for (int t = 0; t < 12; t++) carr[t] = arr[t];
-    HH_TRY(hh_plan3d_create(x, n, n, n, carr, out));
+    HH_TRY(plan3d_create_lines(x, n, n, n, carr, q0, q1, out));
     Plan &p = (*out)->p;
     p.order = order;
     p.src_order = order;
@@ -544,6 +554,10 @@ extern "C" int hh_plan3d_create_helmholtz(hh_ctx *x, int n, int order, double kr
     int rc2 = plan_pade(*out);
     if (rc2 != HH_OK) { hh_plan_destroy(*out); *out = nullptr; return rc2; }
     return HH_OK;
+}
+
+extern "C" int hh_plan3d_create_helmholtz(hh_ctx *x, int n, int order, double kr, double ki, hh_plan **out) {
+    return hh_plan3d_create_helmholtz_lines(x, n, order, kr, ki, 0, (long)n * n, out);
 }
 
 extern "C" int hh_plan_destroy(hh_plan *pl) {
@@ -903,7 +917,29 @@ static int check_batch(hh_plan *pl, int batch) {
         set_error("invalid plan or batch (%d)", batch);
         return HH_ERR_INVALID;
     }
+    if (pl->p.lines_only) {
+        set_error("a line-range plan solves lines only (hh_solve_lines)");
+        return HH_ERR_INVALID;
+    }
     return HH_OK;
+}
+
+// The line solve alone, on right-hand sides already transformed along the other axes: the
+// middle step of hh_solve (fused = 0) or of hh_solve_source (fused = 1, Helmholtz plans).
+extern "C" int hh_solve_lines(hh_plan *pl, const double *in, double *out, int batch, int fused) {
+    if (!pl || batch < 0 || batch > 65535 || (fused != 0 && fused != 1)) {
+        set_error("hh_solve_lines: invalid plan, batch (%d) or fused (%d)", batch, fused);
+        return HH_ERR_INVALID;
+    }
+    if (batch == 0) return HH_OK;
+    if (!in || !out) { set_error("hh_solve_lines: null buffer"); return HH_ERR_INVALID; }
+    Plan &p = pl->p;
+    if (fused && p.src_order == 0) {
+        set_error("hh_solve_lines: the fused operator needs a Helmholtz plan");
+        return HH_ERR_INVALID;
+    }
+    HH_CUDA(cudaSetDevice(p.ctx->device));
+    return launch_line_solve(&p, (const double2 *)in, (double2 *)out, batch, fused ? p.src_order : 0);
 }
 
 extern "C" int hh_solve(hh_plan *pl, const double *rhs, double *sol, int batch) {
@@ -1103,8 +1139,8 @@ extern "C" int hh_solve_source_multi(hh_plan *const *plans, const int *nrhs, int
         if (!plans[i] || nrhs[i] < 0) { set_error("hh_solve_source_multi: plan %d or its count is invalid", i); return HH_ERR_INVALID; }
         ps[(size_t)i] = &plans[i]->p;
         const Plan &a = plans[0]->p, &b = plans[i]->p;
-        if (b.src_order == 0 || b.ctx != a.ctx || b.dim != a.dim || b.nx != a.nx || b.ny != a.ny || b.nz != a.nz ||
-            b.src_order != a.src_order) {
+        if (b.src_order == 0 || b.lines_only || b.ctx != a.ctx || b.dim != a.dim || b.nx != a.nx || b.ny != a.ny ||
+            b.nz != a.nz || b.src_order != a.src_order) {
             set_error("hh_solve_source_multi: plan %d is not a Helmholtz plan of plan 0's shape and context", i);
             return HH_ERR_INVALID;
         }
@@ -1127,7 +1163,8 @@ extern "C" int hh_rhs2d(hh_plan *pl, const hh_rhs2d_data *d, double *rhs) {
 }
 
 extern "C" int hh_rhs3d(hh_plan *pl, const hh_rhs3d_data *d, double *rhs) {
-    if (!pl || !d || !rhs || !d->f_ext || pl->p.dim != 3 || (d->order != 2 && d->order != 4 && d->order != 6) ||
+    if (!pl || !d || !rhs || !d->f_ext || pl->p.dim != 3 || pl->p.lines_only ||
+        (d->order != 2 && d->order != 4 && d->order != 6) ||
         (d->order == 6 && !d->k2_ext) || pl->p.nx < 3 || pl->p.ny < 3 || pl->p.nz < 3 || !(d->hx > 0.0) ||
         !(d->hy > 0.0) || !(d->hz > 0.0)) {
         set_error("hh_rhs3d: invalid arguments (a 3D plan of at least 3^3 points, order 2/4/6, f_ext, k2_ext "

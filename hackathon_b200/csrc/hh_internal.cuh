@@ -138,6 +138,10 @@ struct Plan {
     double   pade_linf = 0.0, pade_uinf = 0.0;     // their common limit (reached from row 9 on)
     double   h = 0.0;
     double2  k2 = {0.0, 0.0};
+    // 3D line-range plans (a rank's pencil of a slab/pencil solve): the plan holds lines
+    // [line0, line0 + lines) of the nx * ny lines and only solves lines (hh_solve_lines)
+    long     line0 = 0;
+    bool     lines_only = false;
 };
 
 // lp: single-precision arithmetic (the refined solve's corrections) where the persistent-warp

@@ -109,6 +109,14 @@ int hh_plan3d_create(hh_ctx *ctx, int nx, int ny, int nz, const double *const co
  * coefficients.c (2D :9-61, 3D :293-389) with k constant. */
 int hh_plan2d_create_helmholtz(hh_ctx *ctx, int n, int order, double k_re, double k_im, hh_plan **out);
 int hh_plan3d_create_helmholtz(hh_ctx *ctx, int n, int order, double k_re, double k_im, hh_plan **out);
+/* One rank's part of a 3D solve split over ranks (no counterpart in the reference, whose solve
+ * runs in one process; the slab/pencil decomposition is that of the paper the reference
+ * accompanies): the z line solves of lines [q0, q1) of the n^2 lines, q = i + j n, laid out
+ * [z][q - q0] per right-hand side (field size (q1 - q0) n).  Such a plan only solves lines
+ * (hh_solve_lines); the other solve entry points, hh_residual, hh_rhs3d and hh_plan_tune refuse
+ * it with HH_ERR_INVALID.  hackathon_b200/slab_pencil.py drives the whole decomposition. */
+int hh_plan3d_create_helmholtz_lines(hh_ctx *ctx, int n, int order, double k_re, double k_im, long q0, long q1,
+                                     hh_plan **out);
 
 int hh_plan_destroy(hh_plan *plan);
 long hh_plan_field_size(const hh_plan *plan);  /* complex values per right-hand side */
@@ -172,6 +180,12 @@ int hh_solve_host(hh_plan *plan, const double *rhs_host, double *sol_host, int b
  * 2D_Program/main_functions/rhs.c:100, 3D_Program/main_functions/rhs.c:198, for this class). */
 int hh_solve_source(hh_plan *plan, const double *f_dev, double *u_dev, int batch);
 int hh_solve_source_host(hh_plan *plan, const double *f_host, double *u_host, int batch);
+/* The line solve alone, on right-hand sides already transformed along the other axes (the
+ * middle step of the reference's solver(): 2D_Program/solver_functions/solver.c:71-86,
+ * 3D_Program/solver_functions/solver.c:483-496): fused = 0 for assembled right-hand sides (as in
+ * hh_solve), 1 for transformed sources with the plan's compact operator (as in hh_solve_source,
+ * Helmholtz plans).  Asynchronous on the plan's stream; in may equal out. */
+int hh_solve_lines(hh_plan *plan, const double *in_dev, double *out_dev, int batch, int fused);
 /* Several wavenumbers in one solve (no counterpart in the reference, which solves one k per
  * run): nplans Helmholtz plans of one shape (dim, n, order) on one context, plan i taking the
  * nrhs[i] consecutive fields of f_dev and u_dev that follow those of plans 0..i-1.  The transforms
