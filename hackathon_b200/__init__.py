@@ -68,6 +68,7 @@ SIGNATURES = {
     "hh_dst1_rows": (_i, [_vp, _i, _l, _vp, _l, _vp, _l]),
     "hh_dst1_cols": (_i, [_vp, _i, _l, _l, _vp, _l, _l, _vp]),
     "hh_dst2_planes": (_i, [_vp, _i, _i, _l, _vp, _vp]),
+    "hh_lines_pack": (_i, [_vp, _vp, _vp, _l, _l, _l, _i, _i]),
     "hh_plan2d_create": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(_vp)]),
     "hh_plan3d_create": (_i, [_vp, _i, _i, _i, C.POINTER(_vp), C.POINTER(_vp)]),
     "hh_plan2d_create_helmholtz": (_i, [_vp, _i, _i, _d, _d, C.POINTER(_vp)]),
@@ -208,6 +209,11 @@ class Context:
 
     def dst1_cols(self, n: int, ncols: int, planes: int, src, ld: int, plane_stride: int, dst):
         check(lib().hh_dst1_cols(self.h, n, ncols, planes, _addr(src), ld, plane_stride, _addr(dst)), "hh_dst1_cols")
+
+    def lines_pack(self, src, dst, batch: int, planes: int, nlines: int, world: int, unpack: bool = False):
+        """hh_lines_pack: a slab [batch][planes][nlines] into the ranks' line parts, or back."""
+        check(lib().hh_lines_pack(self.h, _addr(src), _addr(dst), batch, planes, nlines, world, 1 if unpack else 0),
+              "hh_lines_pack")
 
     def dst2_planes(self, nx: int, ny: int, planes: int, src, dst):
         check(lib().hh_dst2_planes(self.h, nx, ny, planes, _addr(src), _addr(dst)), "hh_dst2_planes")

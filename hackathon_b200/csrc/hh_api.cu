@@ -274,6 +274,16 @@ extern "C" int hh_dst1_cols(hh_ctx *x, int n, long ncols, long planes, const dou
     return launch_dst_cols(&x->c, n, ncols, planes, (const double2 *)in, ld, plane_stride, (double2 *)out);
 }
 
+extern "C" int hh_lines_pack(hh_ctx *x, const double *in, double *out, long batch, long planes, long nlines, int world,
+                             int unpack) {
+    if (!x || !in || !out || in == out || (unpack != 0 && unpack != 1)) {
+        set_error("hh_lines_pack: invalid arguments");
+        return HH_ERR_INVALID;
+    }
+    HH_CUDA(cudaSetDevice(x->c.device));
+    return launch_lines_pack(&x->c, (const double2 *)in, (double2 *)out, batch, planes, nlines, world, unpack == 1);
+}
+
 extern "C" int hh_dst2_planes(hh_ctx *x, int nx, int ny, long nplanes, const double *in, double *out) {
     if (!x || !in || !out || nx < 1 || ny < 1 || nplanes < 0) {
         set_error("hh_dst2_planes: invalid arguments");

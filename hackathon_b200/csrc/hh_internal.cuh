@@ -161,6 +161,9 @@ int launch_dst_cols(Ctx *c, int n, long ncols, long planes, const double2 *in, l
                     double2 *out, bool lp = false, int kern = 0);
 int launch_factor(Plan *p, const double2 *subt, const double2 *diagt, const double2 *supt);
 int launch_line_solve(Plan *p, const double2 *in, double2 *out, int batch, int src_order);
+// slab [batch][planes][nlines] <-> the ranks' line parts of a slab/pencil solve (hh_lines_pack)
+int launch_lines_pack(Ctx *c, const double2 *in, double2 *out, long batch, long planes, long nlines, int world,
+                      bool unpack);
 // one symmetric line-solve launch over several plans of one shape (plan i: nrhs[i] consecutive
 // fields); table_dev holds line_solve_multi_table_bytes(nplans, total) bytes; HH_ERR_UNSUPPORTED
 // (nothing launched) when the plans do not all take the same symmetric kernel variant

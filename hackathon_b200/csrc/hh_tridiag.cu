@@ -584,6 +584,44 @@ int launch_line_solve(Plan *p, const double2 *in, double2 *out, int batch, int s
 
 int segment_count(int rows) { return (rows + kSeg - 1) / kSeg; }
 
+// ------------------------------------------------------------- slab <-> lines ------
+// The cut of transformed planes into the ranks' lines for a slab/pencil solve, and back: element
+// (b, z, q) of a slab [batch][planes][nlines] is element (z, q - q0_s) of rank s's part
+// [planes][cnt_s] of row b of the buffer [batch][planes * nlines], the parts in rank order, for
+// the balanced contiguous split of [0, nlines) over `world` ranks (cnt_s = base + (s < extra),
+// q0_s = s base + min(s, extra)).  One thread per element, consecutive threads on consecutive q.
+__global__ void __launch_bounds__(256) k_lines_pack(const double2 *__restrict__ a, double2 *__restrict__ o,
+                                                    int planes, int nlines, int world, int unpack) {
+    const long row = blockIdx.y; // b * planes + z
+    const long b = row / planes, z = row % planes;
+    const int  base = nlines / world, extra = nlines % world, cut = (base + 1) * extra;
+    const long plane0 = b * (long)planes * nlines;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nlines; q += gridDim.x * blockDim.x) {
+        const int  s = q < cut ? q / (base + 1) : extra + (q - cut) / base;
+        const int  q0 = s * base + min(s, extra), cnt = base + (s < extra ? 1 : 0);
+        const long si = plane0 + z * nlines + q;
+        const long di = plane0 + (long)planes * q0 + z * cnt + (q - q0);
+        if (unpack) o[si] = a[di];
+        else o[di] = a[si];
+    }
+}
+
+int launch_lines_pack(Ctx *c, const double2 *in, double2 *out, long batch, long planes, long nlines, int world,
+                      bool unpack) {
+    if (batch < 0 || planes < 1 || nlines < 1 || world < 1 || world > nlines || batch * planes > 65535 ||
+        nlines > (1L << 30) || planes > (1L << 30)) {
+        set_error("lines pack: batch %ld, planes %ld, lines %ld, ranks %d", batch, planes, nlines, world);
+        return HH_ERR_INVALID;
+    }
+    if (batch == 0) return HH_OK;
+    const long bx = std::min<long>((nlines + 255) / 256, 64);
+    dim3 grid((unsigned)bx, (unsigned)(batch * planes));
+    k_lines_pack<<<grid, 256, 0, c->stream>>>(in, out, (int)planes, (int)nlines, world, unpack ? 1 : 0);
+    HH_CUDA(cudaGetLastError());
+    c->launches++;
+    return HH_OK;
+}
+
 
 // =====================================================================================
 // Symmetric constant-row lines (the Helmholtz plans): k_line_solve_sym
@@ -649,6 +687,14 @@ __device__ __forceinline__ double lds_keep(const double *p) {
 // one column per thread: in registers they would not fit beside the two solves' rows.
 template <int SRC, int KS> struct SymUIS {
     static constexpr bool value = SRC == 6 && KS >= 16;
+};
+// ... and its per-line constants (tau_0, 1/s, c1, cT, c2) in shared memory [5][NT], each read in
+// the sweep that uses it, at the CTA widths where that measured faster with identical bits (line
+// solve, TMA-tile input: 3D 127^3 x 16 0.352 -> 0.317 ms, 255^3 x 4 0.756 -> 0.714 ms, 2D
+// 1023^2 x 64 0.690 -> 0.684 ms; slower at 2 and 8 lines per CTA: 2047^2 x 16 0.851 -> 0.878 ms,
+// 511^2 x 32 0.100 -> 0.103 ms)
+template <int SRC, int KS, int CW> struct SymPCS {
+    static constexpr bool value = SymUIS<SRC, KS>::value && (CW == 4 || CW >= 16);
 };
 
 // Intra-warp inclusive scan of B over the segments of each line in the warp, with the stage
@@ -734,11 +780,15 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
         if constexpr (UIS) return lds_keep(uis + k * NT + t);
         else return ui[k];
     };
-    const double2 tau_in = cmul(s, ui_in); // L_0 = s / P of row r0 - 1
-    const double2 rs = KEEP_L ? s : crcp(s);
+    constexpr bool PCS = SymPCS<SRC, KS, CW>::value;
+    const double2 *pcs = reinterpret_cast<const double2 *>(ttB + (ilog2_t<32 / CW>() + 1) * NT);
+    auto PC = [&](int j) -> double2 { return lds_keep(pcs + j * NT + t); };
+    const double2 tau_in = PCS ? zero : cmul(s, ui_in); // L_0 = s / P of row r0 - 1
+    const double2 rs = PCS ? zero : (KEEP_L ? s : crcp(s));
     // forward multiplier of row r0 + k
     auto LF = [&](int k) -> double2 {
         if constexpr (KEEP_L) return Lr[k];
+        else if constexpr (PCS) return k == 0 ? PC(0) : TV(k - 1);
         else return k == 0 ? tau_in : TV(k - 1);
     };
     // backward multiplier of row r0 + k, tau_k = s ui_k (= L_{k+1} where that row exists)
@@ -819,13 +869,15 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
                 for (int k = 0; k < KS; k++) v[r][k] = cscale(v[r][k], sp.h2);
             } else if constexpr (SRC == 4 || SRC == 6) {
                 double2 prev = gm[r];
+                const double2 c1v = PCS ? PC(2) : c1;
+                const double  c2v = PCS ? PC(4).x : c2;
 #pragma unroll
                 for (int k = 0; k < KS; k++) {
                     const double2 gk = v[r][k], nx = (k == KS - 1) ? gp[r] : v[r][k + 1];
                     const double2 d2 = make_double2(fma(-2.0, gk.x, prev.x + nx.x), fma(-2.0, gk.y, prev.y + nx.y));
                     prev = gk;
                     if constexpr (SRC == 6) g[r][k] = gk;
-                    v[r][k] = zfma(make_double2(c2 * d2.x, c2 * d2.y), c1, gk); // c2 D2 g + c1 g
+                    v[r][k] = zfma(make_double2(c2v * d2.x, c2v * d2.y), c1v, gk); // c2 D2 g + c1 g
                 }
             }
         }
@@ -924,7 +976,8 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
                 if constexpr (SRC == 6) z[r] = zaxpy(bfe[r], aeF, sm.eF[r][w][c]);
             }
             // the rows keep ui_k y_k, so that the back substitution is x_k = ui_k y_k - tau_k x_{k+1}
-            double2 tp = tau_in;
+            double2       tp = PCS ? PC(0) : tau_in;
+            const double2 rsv = PCS ? PC(1) : rs;
 #pragma unroll
             for (int k = 0; k < KS; k++) {
                 double2 u, l;
@@ -933,7 +986,7 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
                     l = Lr[k];
                 } else {
                     const double2 tk = TV(k);
-                    u = cmul(rs, tk);
+                    u = cmul(rsv, tk);
                     l = tp;
                     tp = tk;
                 }
@@ -1017,6 +1070,7 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
             double        aeB = 0.0;
             if constexpr (SRC == 6) aeB = lds_keep(ttB + LOG * NT + t);
             double2 x[NR], ww[NR];
+            const double2 cTv = PCS ? PC(3) : cT;
 #pragma unroll
             for (int r = 0; r < NR; r++) {
                 x[r] = zfma(Bbe[r], AeB, SEQ ? sm.EB[r][w][c] : EB[r]);
@@ -1031,7 +1085,7 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
                     v[r][k] = x[r];
                     if constexpr (SRC == 6) {
                         ww[r] = make_double2(PU(k) * (g[r][k].x - ww[r].x), PU(k) * (g[r][k].y - ww[r].y));
-                        v[r][k] = zfma(v[r][k], cT, ww[r]);
+                        v[r][k] = zfma(v[r][k], cTv, ww[r]);
                     }
                 }
             }
@@ -1041,9 +1095,22 @@ __device__ __forceinline__ void sym_chunk(const double2 *__restrict__ in, double
         for (int r = 0; r < NR; r++) {
             if (b + r >= b_end) break;
             double2 *dst = out + (long)(b + r) * field + off0;
+            if constexpr (PCS) {
+                // one running address and a row count re-formed here: per-row offsets and
+                // conditions hoisted out of the loop over right-hand sides would pin registers
+                long rsd = row_stride;
+                int  nk = live ? rows - r0 : 0;
+                asm volatile("" : "+l"(rsd), "+r"(nk));
 #pragma unroll
-            for (int k = 0; k < KS; k++)
-                if (live && r0 + k < rows) dst[(long)k * row_stride] = v[r][k];
+                for (int k = 0; k < KS; k++) {
+                    if (k < nk) *dst = v[r][k];
+                    dst += rsd;
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < KS; k++)
+                    if (live && r0 + k < rows) dst[(long)k * row_stride] = v[r][k];
+            }
         }
     }
 }
@@ -1218,6 +1285,14 @@ __global__ void __launch_bounds__(NT, MINB)
         c1 = make_double2(sp.h2 * (a6.x - 7.2 * sr.x), sp.h2 * (a6.y - 7.2 * sr.y));
         c2 = sp.h2 * b6;
         cT = make_double2(7.2 * sp.h2 * den.x, 7.2 * sp.h2 * den.y);
+        if constexpr (SymPCS<SRC, KS, CW>::value) {
+            double2 *pcs = reinterpret_cast<double2 *>(ttB + (LOG + 1) * NT);
+            pcs[t] = cmul(s, ui_in);
+            pcs[NT + t] = crcp(s);
+            pcs[2 * NT + t] = c1;
+            pcs[3 * NT + t] = cT;
+            pcs[4 * NT + t] = make_double2(c2, 0.0);
+        }
     }
 
     // ---- scan tables (factor-only, shared by every right-hand side of the chunk)
@@ -1308,7 +1383,8 @@ static int launch_sym_t(Plan *p, const double2 *in, double2 *out, int batch, con
     sp.pu = p->pade_u;
     const int io_elems = TIO ? sym_tile_elems(p->rows, CW) * SymTileBufs<SRC>::value : NR * (KS + 2) * NT;
     const int shm = 128 + (int)(sizeof(double2) * (io_elems + 2 * (LOG + 1) * NT +
-                                                   (SymUIS<SRC, KS>::value ? KS * NT : 0)) +
+                                                   (SymUIS<SRC, KS>::value ? KS * NT : 0) +
+                                                   (SymPCS<SRC, KS, CW>::value ? 5 * NT : 0)) +
                                 (SRC == 6 ? sizeof(double) * 2 * (LOG + 1) * NT : 0));
     CUtensorMap in_map{};
     if constexpr (TIO) HH_TRY(encode_line_map(&in_map, in, p, batch, CW, sym_tile_rows_per_box(p->rows)));

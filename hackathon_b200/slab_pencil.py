@@ -16,16 +16,18 @@ ranks, one per GPU (the decomposition of the paper the reference accompanies, Al
 
 Every plane and every line goes through exactly the arithmetic of the one-process solve, so with
 the same line-solve variant the result is bitwise that of hh_solve_source (or of hh_solve, for
-assembled right-hand sides) on the whole field.  Each exchange is one all_to_all_single over the
-process group (NCCL between GPUs).  The steps of one rank are separate methods, so that a test can
-run several ranks in one process with the exchange done by hand.
+assembled right-hand sides) on the whole field.  Each direction is one all_to_all_single per
+right-hand side over the process group (NCCL between GPUs), laid out so that the forward exchange
+lands in the pencil and the pencil goes back as it is: the only copies are the cut of each
+transformed plane into the ranks' lines before it and the reassembly of the planes after it, one
+kernel each (hh_lines_pack).  The
+steps of one rank are separate methods, so that a test can run several ranks in one process with
+the exchange done by hand.
 """
 
 from __future__ import annotations
 
 import contextlib
-
-import numpy as np
 
 from . import Context, Plan
 
@@ -75,18 +77,40 @@ class DeviceSteps:
         """pencil: [B, n, lines] (z rows of the rank's lines), solved in place."""
         self.plan.solve_lines(pencil, pencil, pencil.shape[0], self.fused)
 
+    def pack(self, slab, send, world: int):
+        """send [B, planes * n^2] <- each plane of slab [B, planes, n, n] cut into the world ranks'
+        lines, the parts in rank order (hh_lines_pack)."""
+        self.ctx.lines_pack(slab, send, slab.shape[0], slab.shape[1], self.n * self.n, world)
+
+    def unpack(self, back, slab, world: int):
+        self.ctx.lines_pack(back, slab, slab.shape[0], slab.shape[1], self.n * self.n, world, unpack=True)
+
     def close(self):
         self.plan.close()
         self.ctx.close()
 
 
 class SlabPencil3D:
-    """Rank `rank` of `world` in a slab/pencil solve of n^3 fields (see the module docstring)."""
+    """Rank `rank` of `world` in a slab/pencil solve of n^3 fields (see the module docstring).
+
+    Exchange buffers, one all_to_all_single per right-hand side and direction:
+
+    * send [B, parts]: right-hand side b's transformed slab, cut into rank s's lines of each
+      plane, [planes][lines_s], for s = 0, 1, ...;
+    * pencil [B, n, lines]: what rank s sends for right-hand side b is rows [z0_s, z1_s) of
+      pencil[b], so the forward exchange lands in place and the pencil goes back as it is;
+    * back [B, parts]: rank s's pencil rows of this rank's planes, [planes][lines_s] for s = 0, 1, ...
+    """
 
     def __init__(self, n: int, rank: int, world: int, steps):
         self.n, self.rank, self.world, self.steps = n, rank, world, steps
         self.zs = split(n, world)
         self.qs = split(n * n, world)
+        z0, z1 = self.zs[rank]
+        q0, q1 = self.qs[rank]
+        # elements per peer in the slab-side buffers (send, back) and in the pencil
+        self.slab_counts = [(z1 - z0) * (b - a) for a, b in self.qs]
+        self.pencil_counts = [(b - a) * (q1 - q0) for a, b in self.zs]
 
     @contextlib.contextmanager
     def _on_steps_stream(self):
@@ -111,71 +135,96 @@ class SlabPencil3D:
     def lines(self) -> tuple[int, int]:
         return self.qs[self.rank]
 
-    # -- the three steps of one rank; chunks are lists indexed by the peer rank
-    def to_pencils(self, f, slab) -> list:
-        """slab <- the transform of the source planes f, both [B, planes, n, n]; chunk s holds rank
-        s's lines of it, [B, planes, lines_s]."""
-        with self._on_steps_stream():
-            self.steps.forward(f, slab)
-            flat = slab.reshape(slab.shape[0], slab.shape[1], self.n * self.n)
-            return [flat[:, :, q0:q1].contiguous() for q0, q1 in self.qs]
+    def _piece(self, buf, b: int, s: int, counts: list, rows: int):
+        off = sum(counts[:s])
+        return buf[b, off:off + counts[s]].view(rows, counts[s] // rows)
 
-    def pencil_shapes(self, batch: int) -> list:
-        q0, q1 = self.lines
-        return [(batch, z1 - z0, q1 - q0) for z0, z1 in self.zs]
+    def send_piece(self, send, b: int, s: int):
+        """Right-hand side b's part of `send` for rank s, [planes][lines_s]."""
+        return self._piece(send, b, s, self.slab_counts, self.planes[1] - self.planes[0])
 
-    def solve_pencil(self, recv: list) -> list:
-        """recv[s]: [B, planes_s, lines] from rank s.  Solves the pencil [B, n, lines]; chunk s
-        holds rank s's planes of it."""
+    def pencil_piece(self, pencil, b: int, s: int):
+        """Rows of rank s's planes in right-hand side b of the pencil, [planes_s][lines]."""
+        z0, z1 = self.zs[s]
+        return pencil[b, z0:z1]
+
+    back_piece = send_piece
+
+    # -- the three steps of one rank
+    def to_pencils(self, f, slab):
+        """slab <- the transform of the source planes f, both [B, planes, n, n]; returns the send
+        buffer."""
         import torch
         with self._on_steps_stream():
-            pencil = torch.cat(recv, dim=1).contiguous()
-            self.steps.lines(pencil)
-            return [pencil[:, z0:z1, :].contiguous() for z0, z1 in self.zs]
+            self.steps.forward(f, slab)
+            send = torch.empty((slab.shape[0], sum(self.slab_counts)), dtype=slab.dtype, device=slab.device)
+            self.steps.pack(slab, send, self.world)
+            return send
 
-    def slab_shapes(self, batch: int) -> list:
-        z0, z1 = self.planes
-        return [(batch, z1 - z0, q1 - q0) for q0, q1 in self.qs]
-
-    def to_slab(self, recv: list, out):
-        """recv[s]: [B, planes, lines_s] from rank s, written into out [B, planes, n, n], which is
-        then transformed back in place."""
+    def new_pencil(self, batch: int, like):
+        import torch
+        q0, q1 = self.lines
         with self._on_steps_stream():
-            flat = out.view(out.shape[0], out.shape[1], self.n * self.n)
-            for (q0, q1), part in zip(self.qs, recv):
-                flat[:, :, q0:q1] = part
+            return torch.empty((batch, self.n, q1 - q0), dtype=like.dtype, device=like.device)
+
+    def new_back(self, batch: int, like):
+        import torch
+        with self._on_steps_stream():
+            return torch.empty((batch, sum(self.slab_counts)), dtype=like.dtype, device=like.device)
+
+    def solve_pencil(self, pencil):
+        """The z line solves of the pencil [B, n, lines], in place."""
+        with self._on_steps_stream():
+            self.steps.lines(pencil)
+
+    def to_slab(self, back, out):
+        """The back buffer into out [B, planes, n, n], which is then transformed back in place."""
+        with self._on_steps_stream():
+            self.steps.unpack(back, out, self.world)
             self.steps.inverse(out)
 
     # -- the whole solve over a process group
     def solve(self, f, u, group=None):
         """u <- the solution's planes of this rank's slab from the source planes f, both
         [B, planes, n, n] complex128 tensors; every rank of the group calls it together."""
-        b = f.shape[0]
+        import torch
+        import torch.distributed as dist
+        nb = f.shape[0]
+        sl = [2 * c for c in self.slab_counts]
+        pc = [2 * c for c in self.pencil_counts]
         with self._on_steps_stream():
-            recv = exchange(self.to_pencils(f, u), self.pencil_shapes(b), group)
-            recv = exchange(self.solve_pencil(recv), self.slab_shapes(b), group)
-            self.to_slab(recv, u)
-
-
-def exchange(chunks: list, recv_shapes: list, group=None) -> list:
-    """One all_to_all_single: chunk s goes to rank s; returns the chunks received, shaped as
-    recv_shapes (complex128)."""
-    import torch
-    import torch.distributed as dist
-    send = torch.cat([torch.view_as_real(c).reshape(-1) for c in chunks])
-    sizes_in = [2 * c.numel() for c in chunks]
-    sizes_out = [2 * int(np.prod(s)) for s in recv_shapes]
-    recv = torch.empty(sum(sizes_out), dtype=torch.float64, device=send.device)
-    dist.all_to_all_single(recv, send, sizes_out, sizes_in, group=group)
-    return [torch.view_as_complex(p.view(*s, 2)) for p, s in zip(torch.split(recv, sizes_out), recv_shapes)]
+            send = self.to_pencils(f, u)
+            pencil = self.new_pencil(nb, u)
+            for b in range(nb):
+                dist.all_to_all_single(torch.view_as_real(pencil[b]).reshape(-1),
+                                       torch.view_as_real(send[b]).reshape(-1), pc, sl, group=group)
+            self.solve_pencil(pencil)
+            back = self.new_back(nb, u)
+            for b in range(nb):
+                dist.all_to_all_single(torch.view_as_real(back[b]).reshape(-1),
+                                       torch.view_as_real(pencil[b]).reshape(-1), sl, pc, group=group)
+            self.to_slab(back, u)
 
 
 def solve_in_process(ranks: list, fs: list, us: list):
     """All ranks of a decomposition in one process, the exchanges done by hand: rank r's slab of
     the sources fs[r] -> us[r].  One GPU (or the CPU) runs the ranks' steps one after another; no
     step of one rank waits for another's."""
-    world = len(ranks)
+    world, nb = len(ranks), fs[0].shape[0]
     sends = [rk.to_pencils(f, u) for rk, f, u in zip(ranks, fs, us)]
-    backs = [rk.solve_pencil([sends[s][r] for s in range(world)]) for r, rk in enumerate(ranks)]
-    for r, (rk, u) in enumerate(zip(ranks, us)):
-        rk.to_slab([backs[s][r] for s in range(world)], u)
+    pencils = [rk.new_pencil(nb, u) for rk, u in zip(ranks, us)]
+    for r, rk in enumerate(ranks):      # receiver
+        for s in range(world):          # sender
+            for b in range(nb):
+                with rk._on_steps_stream():
+                    rk.pencil_piece(pencils[r], b, s).copy_(ranks[s].send_piece(sends[s], b, r))
+    for rk, p in zip(ranks, pencils):
+        rk.solve_pencil(p)
+    backs = [rk.new_back(nb, u) for rk, u in zip(ranks, us)]
+    for r, rk in enumerate(ranks):
+        for s in range(world):
+            for b in range(nb):
+                with rk._on_steps_stream():
+                    rk.back_piece(backs[r], b, s).copy_(ranks[s].pencil_piece(pencils[s], b, r))
+    for rk, bk, u in zip(ranks, backs, us):
+        rk.to_slab(bk, u)

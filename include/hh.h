@@ -91,6 +91,13 @@ int hh_dst1_cols(hh_ctx *ctx, int n, long ncols, long planes, const double *in_d
  * Replaces DST(), 3D_Program/solver_functions/DST.c:148 (one real plane through two FFTW
  * batches and a transpose) and DST1/DST2 (DST.c:13,50). */
 int hh_dst2_planes(hh_ctx *ctx, int nx, int ny, long nplanes, const double *in_dev, double *out_dev);
+/* The exchange layout of a slab/pencil 3D solve (no counterpart in the reference): unpack = 0 cuts
+ * each plane of a slab [batch][planes][nlines] into the parts of the world ranks' lines, row b of
+ * out being [planes][cnt_0], [planes][cnt_1], ... for the balanced contiguous split of the lines
+ * (cnt_s = nlines / world + (s < nlines % world)); unpack = 1 is the inverse.  in and out must not
+ * overlap; batch * planes <= 65535. */
+int hh_lines_pack(hh_ctx *ctx, const double *in_dev, double *out_dev, long batch, long planes, long nlines, int world,
+                  int unpack);
 
 /* ------------------------------------------------------------------ plans ---- */
 /* 2D plan from the reference's per-row 9-point stencil [bm am bm; b a b; bp ap bp]

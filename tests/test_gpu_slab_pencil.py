@@ -60,6 +60,33 @@ def test_ranks_in_one_process_bitwise_one_process_solve(ctx, n, order, k, batch,
     plan.close()
 
 
+@pytest.mark.parametrize("batch,planes,nlines,world", [(3, 5, 961, 3), (1, 32, 65025, 8), (2, 7, 100, 7)])
+def test_lines_pack_layout_and_round_trip(ctx, batch, planes, nlines, world):
+    """hh_lines_pack against torch slicing of the same layout, and unpack(pack(x)) == x."""
+    import torch
+    g = torch.Generator().manual_seed(nlines + world)
+    x = torch.complex(torch.randn((batch, planes, nlines), generator=g, dtype=torch.float64),
+                      torch.randn((batch, planes, nlines), generator=g, dtype=torch.float64)).cuda()
+    send = torch.full((batch, planes * nlines), float("nan"), dtype=torch.complex128, device="cuda")
+    torch.cuda.synchronize()
+    ctx.lines_pack(x, send, batch, planes, nlines, world)
+    ctx.synchronize()
+    off = 0
+    for q0, q1 in SP.split(nlines, world):
+        cnt = planes * (q1 - q0)
+        assert torch.equal(send[:, off:off + cnt].reshape(batch, planes, q1 - q0), x[:, :, q0:q1])
+        off += cnt
+    y = torch.full_like(x, float("nan"))
+    torch.cuda.synchronize()
+    ctx.lines_pack(send, y, batch, planes, nlines, world, unpack=True)
+    ctx.synchronize()
+    assert torch.equal(y, x)
+    with pytest.raises(hh.HHError):
+        ctx.lines_pack(x, x, batch, planes, nlines, world)
+    with pytest.raises(hh.HHError):
+        ctx.lines_pack(x, send, batch, planes, nlines, nlines + 1)
+
+
 def test_line_range_plan_only_solves_lines(ctx):
     import torch
     p = hh.Plan.helmholtz_lines(ctx, 31, 6, 10.0, 100, 500)

@@ -41,6 +41,22 @@ class OracleSteps:
     def inverse(self, slab):
         slab.copy_(torch.from_numpy(np.ascontiguousarray(self._x(self._y(slab.numpy())))))
 
+    def pack(self, slab, send, world):
+        nb, planes = slab.shape[:2]
+        flat, off = slab.reshape(nb, planes, -1), 0
+        for q0, q1 in SP.split(flat.shape[2], world):
+            cnt = planes * (q1 - q0)
+            send[:, off:off + cnt] = flat[:, :, q0:q1].reshape(nb, cnt)
+            off += cnt
+
+    def unpack(self, back, slab, world):
+        nb, planes = slab.shape[:2]
+        flat, off = slab.view(nb, planes, -1), 0
+        for q0, q1 in SP.split(flat.shape[2], world):
+            cnt = planes * (q1 - q0)
+            flat[:, :, q0:q1] = back[:, off:off + cnt].reshape(nb, planes, q1 - q0)
+            off += cnt
+
     def lines(self, pencil):
         p = pencil.numpy()
         nz = p.shape[1]
