@@ -376,6 +376,61 @@ def secondary_configs(hh, ctx, st, torch) -> dict:
     return out
 
 
+def slab_pencil_probe(hh, torch, n: int = 255, batch: int = 4, world: int = 8) -> dict:
+    """One 3D 255^3 x 4 order-6 solve split over `world` slab/pencil ranks (hackathon_b200/
+    slab_pencil.py), the ranks' steps run in turn on this GPU with the exchange done by hand: the
+    time of each rank's own work (CUDA events, best of three) against the one-process solve, and
+    the bitwise check of the assembled result.  Several GPUs would add the all-to-all on top."""
+    from hackathon_b200 import slab_pencil as SP
+    st = torch.cuda.Stream()
+    g = torch.Generator().manual_seed(11)
+    f = torch.complex(torch.randn((batch, n, n, n), generator=g, dtype=torch.float64),
+                      torch.randn((batch, n, n, n), generator=g, dtype=torch.float64)).cuda()
+    ctx = hh.Context(torch.cuda.current_device(), stream=st.cuda_stream)
+    plan = hh.Plan.helmholtz(ctx, 3, n, 6, 30.0)
+
+    def best(fn, reps=3):
+        t = 1e30
+        for _ in range(reps):
+            with torch.cuda.stream(st):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                fn()
+                e1.record(st)
+            e1.synchronize()
+            t = min(t, e0.elapsed_time(e1))
+        return t
+
+    ref = torch.empty_like(f)
+    torch.cuda.synchronize()
+    one = best(lambda: plan.solve_source(f, ref, batch))
+    ranks = [SP.SlabPencil3D(n, r, world, SP.DeviceSteps(torch.cuda.current_device(), n, 6, 30.0,
+                                                         *SP.split(n * n, world)[r], True, plan.variant, st))
+             for r in range(world)]
+    fs = [f[:, rk.planes[0]:rk.planes[1]].contiguous() for rk in ranks]
+    us = [torch.empty_like(x) for x in fs]
+    SP.solve_in_process(ranks, fs, us)
+    torch.cuda.synchronize()
+    same = bool(torch.equal(torch.cat(us, dim=1), ref))
+    r0, nb = ranks[0], batch
+    pen, back = r0.new_pencil(nb, us[0]), r0.new_back(nb, us[0])
+    pen.zero_()
+    back.zero_()
+    t = [best(lambda: r0.to_pencils(fs[0], us[0])), best(lambda: r0.solve_pencil(pen)),
+         best(lambda: r0.to_slab(back, us[0]))]
+    sent = 16 * nb * (sum(r0.slab_counts) - r0.slab_counts[0])
+    for rk in ranks:
+        rk.steps.close()
+    plan.close()
+    ctx.close()
+    del f, ref, fs, us, pen, back
+    torch.cuda.empty_cache()
+    return {"ranks": world, "one_process_ms": one, "rank0_ms": sum(t),
+            "rank0_steps_ms": {"transform_and_cut": t[0], "line_solve": t[1], "reassembly_and_inverse": t[2]},
+            "bytes_rank0_sends_each_way": sent, "bitwise_equal_to_one_process": same,
+            "note": "ranks run in turn on one GPU; the all-to-all between GPUs is not included"}
+
+
 def refined_configs(hh, ctx, st, torch) -> dict:
     """The mixed-precision refined form against the plain FP64 form on the same assembled
     right-hand sides (seeded sine-mode fields used directly as the assembled rhs): 2D N=1023
@@ -793,6 +848,7 @@ def main():
             line["secondary"]["mixed_precision_refined"] = refined_configs(hh, ctx, st, torch)
             line["secondary"]["serving"] = serving_block(hh, torch, seconds=1.0)
             line["secondary"]["dst_as_tensor_core_gemm"] = dst_gemm_probe(torch, st)
+            line["secondary"]["slab_pencil_3d_n255_b4_8_ranks"] = slab_pencil_probe(hh, torch)
         def gpu_solve(order, k, f_int):
             return plans[COMBOS.index((order, k))].solve_source_host(f_int)
 
