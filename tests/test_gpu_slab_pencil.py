@@ -32,8 +32,8 @@ def _ranks(n, order, k, world, fused, variant):
     return out
 
 
-@pytest.mark.parametrize("n,order,k,batch", [(31, 6, 10.0, 3), (63, 4, 30.0, 2), (127, 6, 30.0, 2),
-                                             (255, 6, 30.0, 1)])
+@pytest.mark.parametrize("n,order,k,batch", [(31, 6, 10.0, 3), (63, 4, 30.0, 2), (47, 2, 20.0, 2),
+                                             (127, 6, 30.0, 2), (255, 6, 30.0, 1)])
 @pytest.mark.parametrize("world", [2, 3, 8])
 @pytest.mark.parametrize("fused", [True, False])
 def test_ranks_in_one_process_bitwise_one_process_solve(ctx, n, order, k, batch, world, fused):
