@@ -431,6 +431,99 @@ def slab_pencil_probe(hh, torch, n: int = 255, batch: int = 4, world: int = 8) -
             "note": "ranks run in turn on one GPU; the all-to-all between GPUs is not included"}
 
 
+def run_slab_pencil(args, rank: int, world: int, local: int) -> None:
+    """One 3D solve split over the job's GPUs (hackathon_b200/slab_pencil.py): rank r holds its
+    slab of a 255^3 x 4 field, order 6, k = 30, and the exchange is NCCL's all_to_all_single.
+    Times K solves after W warm-up ones (barrier and CUDA events around them, max over ranks) and
+    checks the result against a one-process solve on rank 0 through a sum of |u|^2 over the
+    slabs.  Strong scaling: the field is the same at every N."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    import hackathon_b200 as hh
+    from hackathon_b200 import slab_pencil as SP
+    n, order, k, batch = 255, 6, 30.0, 4
+    torch.cuda.set_device(local)
+    if "MASTER_ADDR" not in os.environ:  # a single process without torchrun
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(sk.getsockname()[1])
+    dist.init_process_group("nccl", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device("cuda", local))
+    z0, z1 = SP.split(n, world)[rank]
+    q0, q1 = SP.split(n * n, world)[rank]
+
+    def planes(a, b):  # the field's planes [a, b) of every right-hand side, seeded per plane
+        out = torch.empty((batch, b - a, n, n), dtype=torch.complex128, device="cuda")
+        for r in range(batch):
+            for z in range(a, b):
+                g = torch.Generator(device="cuda").manual_seed(1_000_003 * r + z)
+                out[r, z - a] = torch.randn((n, n), generator=g, dtype=torch.complex128, device="cuda")
+        return out
+
+    f = planes(z0, z1)
+    u = torch.empty_like(f)
+    variant = None
+    if rank == 0:
+        ctx0 = hh.Context(local)
+        p0 = hh.Plan.helmholtz(ctx0, 3, n, order, k)
+        variant = p0.variant
+        p0.close()
+        ctx0.close()
+    vt = torch.tensor([variant if variant is not None else -1], device="cuda")
+    dist.broadcast(vt, 0)
+    rk = SP.SlabPencil3D(n, rank, world, SP.DeviceSteps(local, n, order, k, q0, q1, True, int(vt.item())))
+    for _ in range(args.warmup):
+        rk.solve(f, u)
+    torch.cuda.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        rk.solve(f, u)
+    e1.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    ms = torch.tensor([e0.elapsed_time(e1) / args.steps], device="cuda", dtype=torch.float64)
+    dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    sq = torch.tensor([float((u.abs() ** 2).sum().item())], device="cuda", dtype=torch.float64)
+    dist.all_reduce(sq)
+    line = None
+    if rank == 0:
+        st1 = torch.cuda.Stream()
+        ctx1 = hh.Context(local, stream=st1.cuda_stream)
+        p1 = hh.Plan.helmholtz(ctx1, 3, n, order, k)
+        full = planes(0, n)
+        ref = torch.empty_like(full)
+        torch.cuda.synchronize()
+        p1.solve_source(full, ref, batch)
+        ctx1.synchronize()
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record(st1)
+        for _ in range(args.steps):
+            p1.solve_source(full, ref, batch)
+        e3.record(st1)
+        e3.synchronize()
+        one = e2.elapsed_time(e3) / args.steps
+        sq_ref = float((ref.abs() ** 2).sum().item())
+        t = float(ms.item())
+        line = {"metric": "one 3D 255^3 x 4 order-6 solve split over the job's GPUs (slab/pencil, NCCL all-to-all)",
+                "value": batch / (t / 1000.0), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True, "scaling": "strong",
+                "mode": "slab_pencil", "one_gpu_ms_per_step": one,
+                "sum_abs2_rel_diff_vs_one_process": abs(float(sq.item()) - sq_ref) / sq_ref,
+                "timing": "CUDA events around K solves on each rank, max over ranks"}
+        p1.close()
+        ctx1.close()
+    rk.steps.close()
+    dist.barrier()
+    dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
 def refined_configs(hh, ctx, st, torch) -> dict:
     """The mixed-precision refined form against the plain FP64 form on the same assembled
     right-hand sides (seeded sine-mode fields used directly as the assembled rhs): 2D N=1023
@@ -656,6 +749,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the 3D 255^3 and 2D 2047^2 figures")
     ap.add_argument("--serve", action="store_true", help="run only the serving configuration and print its line")
+    ap.add_argument("--slab-pencil", action="store_true",
+                    help="one 3D 255^3 x 4 solve split over the job's GPUs (strong scaling) instead of the replicas")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--batch", type=int, default=BATCH, help="right-hand sides per step (profiling runs)")
@@ -674,6 +769,10 @@ def main():
     import torch.distributed as dist
 
     import hackathon_b200 as hh
+
+    if args.slab_pencil:
+        run_slab_pencil(args, rank, world, local)
+        return
 
     if args.serve:
         if rank == 0:
