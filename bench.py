@@ -418,7 +418,8 @@ def slab_pencil_probe(hh, torch, n: int = 255, batch: int = 4, world: int = 8) -
     back.zero_()
     t = [best(lambda: r0.to_pencils(fs[0], us[0])), best(lambda: r0.solve_pencil(pen)),
          best(lambda: r0.to_slab(back, us[0]))]
-    sent = 16 * nb * (sum(r0.slab_counts) - r0.slab_counts[0])
+    counts = r0.slab_counts(nb)
+    sent = 16 * (sum(counts) - counts[0])
     for rk in ranks:
         rk.steps.close()
     plan.close()

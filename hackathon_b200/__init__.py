@@ -95,6 +95,7 @@ SIGNATURES = {
     "hh_solve_source": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source_host": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_lines": (_i, [_vp, _vp, _vp, _i, _i]),
+    "hh_solve_lines_strided": (_i, [_vp, _vp, _vp, _i, _i, _l, _l]),
     "hh_solve_source_host_noalloc": (_i, [_vp, _vp, _vp, _i]),
     "hh_solve_source_multi": (_i, [C.POINTER(_vp), C.POINTER(_i), _i, _vp, _vp]),
     "hh_rhs2d": (_i, [_vp, C.POINTER(Rhs2DData), _vp]),
@@ -336,6 +337,11 @@ class Plan:
         """The line solve alone on transformed fields (hh_solve_lines): fused = True for transformed
         sources (the Helmholtz plans' compact operator), False for assembled right-hand sides."""
         check(lib().hh_solve_lines(self.h, _addr(src), _addr(dst), batch, 1 if fused else 0), "hh_solve_lines")
+
+    def solve_lines_strided(self, src, dst, batch: int, fused: bool, row_stride: int, field: int):
+        """hh_solve_lines_strided: the line solve over fields at b field + r row_stride + q."""
+        check(lib().hh_solve_lines_strided(self.h, _addr(src), _addr(dst), batch, 1 if fused else 0, row_stride,
+                                           field), "hh_solve_lines_strided")
 
     def solve_refined(self, rhs, sol, batch: int = 1, tol: float = 1e-10, max_iter: int = 10):
         """hh_solve_refined on device buffers; returns (corrections, relative residual)."""

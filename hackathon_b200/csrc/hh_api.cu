@@ -935,8 +935,10 @@ static int check_batch(hh_plan *pl, int batch) {
 }
 
 // The line solve alone, on right-hand sides already transformed along the other axes: the
-// middle step of hh_solve (fused = 0) or of hh_solve_source (fused = 1, Helmholtz plans).
-extern "C" int hh_solve_lines(hh_plan *pl, const double *in, double *out, int batch, int fused) {
+// middle step of hh_solve (fused = 0) or of hh_solve_source (fused = 1, Helmholtz plans), with
+// element (row r, line q) of right-hand side b at b field + r row_stride + q.
+extern "C" int hh_solve_lines_strided(hh_plan *pl, const double *in, double *out, int batch, int fused, long row_stride,
+                                      long field) {
     if (!pl || batch < 0 || batch > 65535 || (fused != 0 && fused != 1)) {
         set_error("hh_solve_lines: invalid plan, batch (%d) or fused (%d)", batch, fused);
         return HH_ERR_INVALID;
@@ -948,8 +950,25 @@ extern "C" int hh_solve_lines(hh_plan *pl, const double *in, double *out, int ba
         set_error("hh_solve_lines: the fused operator needs a Helmholtz plan");
         return HH_ERR_INVALID;
     }
+    // the fields either follow each other (field >= rows row_stride) or interleave row by row
+    // (row_stride >= batch field); lines are contiguous either way
+    const bool rhs_major = row_stride >= p.lines && field >= (long)p.rows * row_stride;
+    const bool row_major = field >= p.lines && row_stride >= (long)batch * field;
+    if (!rhs_major && !row_major) {
+        set_error("hh_solve_lines: overlapping layout (row stride %ld, field %ld, %d lines of %d rows, batch %d)",
+                  row_stride, field, p.lines, p.rows, batch);
+        return HH_ERR_INVALID;
+    }
     HH_CUDA(cudaSetDevice(p.ctx->device));
-    return launch_line_solve(&p, (const double2 *)in, (double2 *)out, batch, fused ? p.src_order : 0);
+    Plan q = p; // the same factors and tables over another layout of the fields
+    q.row_stride = row_stride;
+    q.field = field;
+    return launch_line_solve(&q, (const double2 *)in, (double2 *)out, batch, fused ? p.src_order : 0);
+}
+
+extern "C" int hh_solve_lines(hh_plan *pl, const double *in, double *out, int batch, int fused) {
+    if (!pl) { set_error("hh_solve_lines: invalid plan"); return HH_ERR_INVALID; }
+    return hh_solve_lines_strided(pl, in, out, batch, fused, pl->p.row_stride, pl->p.field);
 }
 
 extern "C" int hh_solve(hh_plan *pl, const double *rhs, double *sol, int batch) {

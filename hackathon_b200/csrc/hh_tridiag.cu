@@ -586,21 +586,20 @@ int segment_count(int rows) { return (rows + kSeg - 1) / kSeg; }
 
 // ------------------------------------------------------------- slab <-> lines ------
 // The cut of transformed planes into the ranks' lines for a slab/pencil solve, and back: element
-// (b, z, q) of a slab [batch][planes][nlines] is element (z, q - q0_s) of rank s's part
-// [planes][cnt_s] of row b of the buffer [batch][planes * nlines], the parts in rank order, for
-// the balanced contiguous split of [0, nlines) over `world` ranks (cnt_s = base + (s < extra),
-// q0_s = s base + min(s, extra)).  One thread per element, consecutive threads on consecutive q.
+// (b, z, q) of a slab [batch][planes][nlines] is element (z, b, q - q0_s) of rank s's part
+// [planes][batch][cnt_s] of the buffer, the parts in rank order, for the balanced contiguous
+// split of [0, nlines) over `world` ranks (cnt_s = base + (s < extra), q0_s = s base +
+// min(s, extra)).  One thread per element, consecutive threads on consecutive q.
 __global__ void __launch_bounds__(256) k_lines_pack(const double2 *__restrict__ a, double2 *__restrict__ o,
-                                                    int planes, int nlines, int world, int unpack) {
+                                                    int batch, int planes, int nlines, int world, int unpack) {
     const long row = blockIdx.y; // b * planes + z
     const long b = row / planes, z = row % planes;
     const int  base = nlines / world, extra = nlines % world, cut = (base + 1) * extra;
-    const long plane0 = b * (long)planes * nlines;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nlines; q += gridDim.x * blockDim.x) {
         const int  s = q < cut ? q / (base + 1) : extra + (q - cut) / base;
         const int  q0 = s * base + min(s, extra), cnt = base + (s < extra ? 1 : 0);
-        const long si = plane0 + z * nlines + q;
-        const long di = plane0 + (long)planes * q0 + z * cnt + (q - q0);
+        const long si = row * nlines + q;
+        const long di = (long)batch * planes * q0 + (z * batch + b) * cnt + (q - q0);
         if (unpack) o[si] = a[di];
         else o[di] = a[si];
     }
@@ -616,7 +615,7 @@ int launch_lines_pack(Ctx *c, const double2 *in, double2 *out, long batch, long 
     if (batch == 0) return HH_OK;
     const long bx = std::min<long>((nlines + 255) / 256, 64);
     dim3 grid((unsigned)bx, (unsigned)(batch * planes));
-    k_lines_pack<<<grid, 256, 0, c->stream>>>(in, out, (int)planes, (int)nlines, world, unpack ? 1 : 0);
+    k_lines_pack<<<grid, 256, 0, c->stream>>>(in, out, (int)batch, (int)planes, (int)nlines, world, unpack ? 1 : 0);
     HH_CUDA(cudaGetLastError());
     c->launches++;
     return HH_OK;

@@ -16,11 +16,12 @@ ranks, one per GPU (the decomposition of the paper the reference accompanies, Al
 
 Every plane and every line goes through exactly the arithmetic of the one-process solve, so with
 the same line-solve variant the result is bitwise that of hh_solve_source (or of hh_solve, for
-assembled right-hand sides) on the whole field.  Each direction is one all_to_all_single per
-right-hand side over the process group (NCCL between GPUs), laid out so that the forward exchange
-lands in the pencil and the pencil goes back as it is: the only copies are the cut of each
-transformed plane into the ranks' lines before it and the reassembly of the planes after it, one
-kernel each (hh_lines_pack).  The
+assembled right-hand sides) on the whole field.  Each direction is one all_to_all_single for the
+whole batch over the process group (NCCL between GPUs), laid out so that the forward exchange
+lands in the pencil and the pencil goes back as it is: the pencil interleaves the right-hand
+sides row by row ([z][b][line], solved by hh_solve_lines_strided), and the only copies are the
+cut of the transformed slab into the ranks' lines before the exchange and the reassembly of the
+planes after it, one kernel each (hh_lines_pack).  The
 steps of one rank are separate methods, so that a test can run several ranks in one process with
 the exchange done by hand.
 """
@@ -74,12 +75,14 @@ class DeviceSteps:
         self.ctx.dst1_rows(n, planes * n, slab, slab)
 
     def lines(self, pencil):
-        """pencil: [B, n, lines] (z rows of the rank's lines), solved in place."""
-        self.plan.solve_lines(pencil, pencil, pencil.shape[0], self.fused)
+        """pencil: [n, B, lines] (z rows of the rank's lines, right-hand sides interleaved row by
+        row), solved in place."""
+        nb, cnt = pencil.shape[1], pencil.shape[2]
+        self.plan.solve_lines_strided(pencil, pencil, nb, self.fused, nb * cnt, cnt)
 
     def pack(self, slab, send, world: int):
-        """send [B, planes * n^2] <- each plane of slab [B, planes, n, n] cut into the world ranks'
-        lines, the parts in rank order (hh_lines_pack)."""
+        """send <- slab [B, planes, n, n] cut into the world ranks' lines, rank s's part
+        [planes][B][lines_s], the parts in rank order (hh_lines_pack)."""
         self.ctx.lines_pack(slab, send, slab.shape[0], slab.shape[1], self.n * self.n, world)
 
     def unpack(self, back, slab, world: int):
@@ -93,24 +96,20 @@ class DeviceSteps:
 class SlabPencil3D:
     """Rank `rank` of `world` in a slab/pencil solve of n^3 fields (see the module docstring).
 
-    Exchange buffers, one all_to_all_single per right-hand side and direction:
+    Exchange buffers, one all_to_all_single each way for the whole batch of B right-hand sides:
 
-    * send [B, parts]: right-hand side b's transformed slab, cut into rank s's lines of each
-      plane, [planes][lines_s], for s = 0, 1, ...;
-    * pencil [B, n, lines]: what rank s sends for right-hand side b is rows [z0_s, z1_s) of
-      pencil[b], so the forward exchange lands in place and the pencil goes back as it is;
-    * back [B, parts]: rank s's pencil rows of this rank's planes, [planes][lines_s] for s = 0, 1, ...
+    * send: the transformed slab cut into the ranks' lines, rank s's part [planes][B][lines_s],
+      the parts in rank order;
+    * pencil [n, B, lines]: the z rows of this rank's lines, right-hand sides interleaved row by
+      row, so that what rank s sends is rows [z0_s, z1_s), contiguous: the forward exchange lands
+      in place and the pencil goes back as it is;
+    * back: rank s's pencil rows of this rank's planes, [planes][B][lines_s], in rank order.
     """
 
     def __init__(self, n: int, rank: int, world: int, steps):
         self.n, self.rank, self.world, self.steps = n, rank, world, steps
         self.zs = split(n, world)
         self.qs = split(n * n, world)
-        z0, z1 = self.zs[rank]
-        q0, q1 = self.qs[rank]
-        # elements per peer in the slab-side buffers (send, back) and in the pencil
-        self.slab_counts = [(z1 - z0) * (b - a) for a, b in self.qs]
-        self.pencil_counts = [(b - a) * (q1 - q0) for a, b in self.zs]
 
     @contextlib.contextmanager
     def _on_steps_stream(self):
@@ -135,20 +134,29 @@ class SlabPencil3D:
     def lines(self) -> tuple[int, int]:
         return self.qs[self.rank]
 
-    def _piece(self, buf, b: int, s: int, counts: list, rows: int):
+    def slab_counts(self, batch: int) -> list:
+        """Elements per peer in the slab-side buffers (send, back)."""
+        z0, z1 = self.planes
+        return [(z1 - z0) * batch * (b - a) for a, b in self.qs]
+
+    def pencil_counts(self, batch: int) -> list:
+        """Elements per peer in the pencil."""
+        q0, q1 = self.lines
+        return [(b - a) * batch * (q1 - q0) for a, b in self.zs]
+
+    def send_piece(self, send, s: int, batch: int):
+        """Rank s's part of a send (or back) buffer, [planes][B][lines_s]."""
+        counts = self.slab_counts(batch)
         off = sum(counts[:s])
-        return buf[b, off:off + counts[s]].view(rows, counts[s] // rows)
-
-    def send_piece(self, send, b: int, s: int):
-        """Right-hand side b's part of `send` for rank s, [planes][lines_s]."""
-        return self._piece(send, b, s, self.slab_counts, self.planes[1] - self.planes[0])
-
-    def pencil_piece(self, pencil, b: int, s: int):
-        """Rows of rank s's planes in right-hand side b of the pencil, [planes_s][lines]."""
-        z0, z1 = self.zs[s]
-        return pencil[b, z0:z1]
+        q0, q1 = self.qs[s]
+        return send[off:off + counts[s]].view(self.planes[1] - self.planes[0], batch, q1 - q0)
 
     back_piece = send_piece
+
+    def pencil_piece(self, pencil, s: int):
+        """Rows of rank s's planes in the pencil, [planes_s][B][lines]."""
+        z0, z1 = self.zs[s]
+        return pencil[z0:z1]
 
     # -- the three steps of one rank
     def to_pencils(self, f, slab):
@@ -157,7 +165,7 @@ class SlabPencil3D:
         import torch
         with self._on_steps_stream():
             self.steps.forward(f, slab)
-            send = torch.empty((slab.shape[0], sum(self.slab_counts)), dtype=slab.dtype, device=slab.device)
+            send = torch.empty(sum(self.slab_counts(slab.shape[0])), dtype=slab.dtype, device=slab.device)
             self.steps.pack(slab, send, self.world)
             return send
 
@@ -165,15 +173,15 @@ class SlabPencil3D:
         import torch
         q0, q1 = self.lines
         with self._on_steps_stream():
-            return torch.empty((batch, self.n, q1 - q0), dtype=like.dtype, device=like.device)
+            return torch.empty((self.n, batch, q1 - q0), dtype=like.dtype, device=like.device)
 
     def new_back(self, batch: int, like):
         import torch
         with self._on_steps_stream():
-            return torch.empty((batch, sum(self.slab_counts)), dtype=like.dtype, device=like.device)
+            return torch.empty(sum(self.slab_counts(batch)), dtype=like.dtype, device=like.device)
 
     def solve_pencil(self, pencil):
-        """The z line solves of the pencil [B, n, lines], in place."""
+        """The z line solves of the pencil [n, B, lines], in place."""
         with self._on_steps_stream():
             self.steps.lines(pencil)
 
@@ -190,19 +198,17 @@ class SlabPencil3D:
         import torch
         import torch.distributed as dist
         nb = f.shape[0]
-        sl = [2 * c for c in self.slab_counts]
-        pc = [2 * c for c in self.pencil_counts]
+        sl = [2 * c for c in self.slab_counts(nb)]
+        pc = [2 * c for c in self.pencil_counts(nb)]
         with self._on_steps_stream():
             send = self.to_pencils(f, u)
             pencil = self.new_pencil(nb, u)
-            for b in range(nb):
-                dist.all_to_all_single(torch.view_as_real(pencil[b]).reshape(-1),
-                                       torch.view_as_real(send[b]).reshape(-1), pc, sl, group=group)
+            dist.all_to_all_single(torch.view_as_real(pencil).reshape(-1), torch.view_as_real(send).reshape(-1),
+                                   pc, sl, group=group)
             self.solve_pencil(pencil)
             back = self.new_back(nb, u)
-            for b in range(nb):
-                dist.all_to_all_single(torch.view_as_real(back[b]).reshape(-1),
-                                       torch.view_as_real(pencil[b]).reshape(-1), sl, pc, group=group)
+            dist.all_to_all_single(torch.view_as_real(back).reshape(-1), torch.view_as_real(pencil).reshape(-1),
+                                   sl, pc, group=group)
             self.to_slab(back, u)
 
 
@@ -215,16 +221,14 @@ def solve_in_process(ranks: list, fs: list, us: list):
     pencils = [rk.new_pencil(nb, u) for rk, u in zip(ranks, us)]
     for r, rk in enumerate(ranks):      # receiver
         for s in range(world):          # sender
-            for b in range(nb):
-                with rk._on_steps_stream():
-                    rk.pencil_piece(pencils[r], b, s).copy_(ranks[s].send_piece(sends[s], b, r))
+            with rk._on_steps_stream():
+                rk.pencil_piece(pencils[r], s).copy_(ranks[s].send_piece(sends[s], r, nb))
     for rk, p in zip(ranks, pencils):
         rk.solve_pencil(p)
     backs = [rk.new_back(nb, u) for rk, u in zip(ranks, us)]
     for r, rk in enumerate(ranks):
         for s in range(world):
-            for b in range(nb):
-                with rk._on_steps_stream():
-                    rk.back_piece(backs[r], b, s).copy_(ranks[s].pencil_piece(pencils[s], b, r))
+            with rk._on_steps_stream():
+                rk.back_piece(backs[r], s, nb).copy_(ranks[s].pencil_piece(pencils[s], r))
     for rk, bk, u in zip(ranks, backs, us):
         rk.to_slab(bk, u)

@@ -92,10 +92,10 @@ int hh_dst1_cols(hh_ctx *ctx, int n, long ncols, long planes, const double *in_d
  * batches and a transpose) and DST1/DST2 (DST.c:13,50). */
 int hh_dst2_planes(hh_ctx *ctx, int nx, int ny, long nplanes, const double *in_dev, double *out_dev);
 /* The exchange layout of a slab/pencil 3D solve (no counterpart in the reference): unpack = 0 cuts
- * each plane of a slab [batch][planes][nlines] into the parts of the world ranks' lines, row b of
- * out being [planes][cnt_0], [planes][cnt_1], ... for the balanced contiguous split of the lines
- * (cnt_s = nlines / world + (s < nlines % world)); unpack = 1 is the inverse.  in and out must not
- * overlap; batch * planes <= 65535. */
+ * a slab [batch][planes][nlines] into the parts of the world ranks' lines, out being
+ * [planes][batch][cnt_0], [planes][batch][cnt_1], ... for the balanced contiguous split of the
+ * lines (cnt_s = nlines / world + (s < nlines % world)); unpack = 1 is the inverse.  in and out
+ * must not overlap; batch * planes <= 65535. */
 int hh_lines_pack(hh_ctx *ctx, const double *in_dev, double *out_dev, long batch, long planes, long nlines, int world,
                   int unpack);
 
@@ -193,6 +193,12 @@ int hh_solve_source_host(hh_plan *plan, const double *f_host, double *u_host, in
  * hh_solve), 1 for transformed sources with the plan's compact operator (as in hh_solve_source,
  * Helmholtz plans).  Asynchronous on the plan's stream; in may equal out. */
 int hh_solve_lines(hh_plan *plan, const double *in_dev, double *out_dev, int batch, int fused);
+/* The same over another layout: element (row r, line q) of right-hand side b at
+ * b field + r row_stride + q, the fields either one after another (field >= rows row_stride) or
+ * interleaved row by row (row_stride >= batch field, e.g. a pencil [row][b][line]); lines are
+ * contiguous.  Other layouts fail with HH_ERR_INVALID. */
+int hh_solve_lines_strided(hh_plan *plan, const double *in_dev, double *out_dev, int batch, int fused,
+                           long row_stride, long field);
 /* Several wavenumbers in one solve (no counterpart in the reference, which solves one k per
  * run): nplans Helmholtz plans of one shape (dim, n, order) on one context, plan i taking the
  * nrhs[i] consecutive fields of f_dev and u_dev that follow those of plans 0..i-1.  The transforms

@@ -67,14 +67,14 @@ def test_lines_pack_layout_and_round_trip(ctx, batch, planes, nlines, world):
     g = torch.Generator().manual_seed(nlines + world)
     x = torch.complex(torch.randn((batch, planes, nlines), generator=g, dtype=torch.float64),
                       torch.randn((batch, planes, nlines), generator=g, dtype=torch.float64)).cuda()
-    send = torch.full((batch, planes * nlines), float("nan"), dtype=torch.complex128, device="cuda")
+    send = torch.full((batch * planes * nlines,), float("nan"), dtype=torch.complex128, device="cuda")
     torch.cuda.synchronize()
     ctx.lines_pack(x, send, batch, planes, nlines, world)
     ctx.synchronize()
     off = 0
-    for q0, q1 in SP.split(nlines, world):
-        cnt = planes * (q1 - q0)
-        assert torch.equal(send[:, off:off + cnt].reshape(batch, planes, q1 - q0), x[:, :, q0:q1])
+    for q0, q1 in SP.split(nlines, world):  # rank s's part [planes][batch][lines_s]
+        cnt = planes * batch * (q1 - q0)
+        assert torch.equal(send[off:off + cnt].reshape(planes, batch, q1 - q0), x[:, :, q0:q1].permute(1, 0, 2))
         off += cnt
     y = torch.full_like(x, float("nan"))
     torch.cuda.synchronize()
@@ -85,6 +85,29 @@ def test_lines_pack_layout_and_round_trip(ctx, batch, planes, nlines, world):
         ctx.lines_pack(x, x, batch, planes, nlines, world)
     with pytest.raises(hh.HHError):
         ctx.lines_pack(x, send, batch, planes, nlines, nlines + 1)
+
+
+def test_strided_line_solve_interleaved_equals_contiguous(ctx):
+    """hh_solve_lines_strided on fields interleaved row by row ([z][b][line]) gives the bits of
+    hh_solve_lines on the same fields one after another ([b][z][line]); overlapping layouts are
+    refused."""
+    import torch
+    n, batch = 63, 3
+    g = torch.Generator().manual_seed(63)
+    f = torch.complex(torch.randn((batch, n, n * n), generator=g, dtype=torch.float64),
+                      torch.randn((batch, n, n * n), generator=g, dtype=torch.float64)).cuda()
+    p = hh.Plan.helmholtz(ctx, 3, n, 6, 20.0)
+    a = f.clone()
+    b = f.permute(1, 0, 2).contiguous()
+    torch.cuda.synchronize()
+    p.solve_lines(a, a, batch)
+    p.solve_lines_strided(b, b, batch, True, batch * n * n, n * n)
+    ctx.synchronize()
+    assert torch.isfinite(a).all()
+    assert torch.equal(b.permute(1, 0, 2), a)
+    with pytest.raises(hh.HHError):
+        p.solve_lines_strided(b, b, batch, True, n * n, n * n)  # fields would overlap
+    p.close()
 
 
 def test_line_range_plan_only_solves_lines(ctx):

@@ -45,23 +45,23 @@ class OracleSteps:
         nb, planes = slab.shape[:2]
         flat, off = slab.reshape(nb, planes, -1), 0
         for q0, q1 in SP.split(flat.shape[2], world):
-            cnt = planes * (q1 - q0)
-            send[:, off:off + cnt] = flat[:, :, q0:q1].reshape(nb, cnt)
+            cnt = planes * nb * (q1 - q0)
+            send[off:off + cnt] = flat[:, :, q0:q1].permute(1, 0, 2).reshape(cnt)
             off += cnt
 
     def unpack(self, back, slab, world):
         nb, planes = slab.shape[:2]
         flat, off = slab.view(nb, planes, -1), 0
         for q0, q1 in SP.split(flat.shape[2], world):
-            cnt = planes * (q1 - q0)
-            flat[:, :, q0:q1] = back[:, off:off + cnt].reshape(nb, planes, q1 - q0)
+            cnt = planes * nb * (q1 - q0)
+            flat[:, :, q0:q1] = back[off:off + cnt].reshape(planes, nb, q1 - q0).permute(1, 0, 2)
             off += cnt
 
     def lines(self, pencil):
-        p = pencil.numpy()
-        nz = p.shape[1]
-        for b in range(p.shape[0]):
-            r = p[b]
+        p = pencil.numpy()  # [z][b][line]
+        nz = p.shape[0]
+        for b in range(p.shape[1]):
+            r = p[:, b]
             y = np.empty_like(r)
             y[0] = r[0]
             for l in range(1, nz):
@@ -70,7 +70,7 @@ class OracleSteps:
             x[nz - 1] = y[nz - 1] * self.U[nz - 1]
             for l in range(nz - 2, -1, -1):
                 x[l] = (y[l] - self.Up[l] * x[l + 1]) * self.U[l]
-            p[b] = x
+            p[:, b] = x
 
 
 def _problem(n, order, k, batch):
